@@ -1,0 +1,311 @@
+#!/usr/bin/env python3
+"""Benchmark: batched independent partial-order alignments on B200.
+
+Workload (default): 4,096 independent read sets, ancestor length log-uniform
+in 200-5,000 bp, depth uniform in 10-60 reads, per-set error uniform in
+2-15% split 60/20/20 among substitution / insertion / deletion (seed 1003);
+default Params (static band b=100, f=40), i32 DP. A step is one full pass
+of the read loop over every set (Graph::new, then align -> add_path ->
+toposort for each read), all resident on the GPU.
+
+Metric: GCUPS = 8-aligned band cells computed (retries included) / s / 1e9.
+`value` is device time of the batched run with inputs already in HBM; `e2e`
+goes through the C ABI from host buffers (upload, run, download and render
+every set's consensus). The CPU baseline is the oracle's 8-lane AVX2 kernel
+on the host's threads over a bounded sample of the same sets.
+
+Multi-GPU: one process per GPU, each aligning its own 4,096 sets (weak
+scaling, no collective on the data path); value = all ranks' cells / the
+slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "minipoa-rs_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+WORKLOAD = ("batched independent POA: 4096 read sets, ancestor 200-5000 bp log-uniform, depth 10-60, "
+            "error 2-15% (60/20/20 sub/ins/del), default Params, consensus output")
+METRIC = "GCUPS (batched POA, bit-exact)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sets", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=1003)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-sets", type=int, default=64, help="sets timed in the plain per-read form")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_baseline(sets, params, seconds: float):
+    """Oracle AVX2 kernel on all host threads over a bounded sample of the
+    same sets (taken in set order until about `seconds` of CPU time)."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    done_cells, done_sets, elapsed = 0, 0, 0.0
+    chunk = max(threads, 8)
+    i = 0
+    while i < len(sets) and elapsed < seconds:
+        part = sets[i:i + chunk]
+        t0 = time.perf_counter()
+        cells, _ = oracle.batch_run(params, part, kernel=oracle.AUTO_AVX2, threads=threads, out_format=0)
+        elapsed += time.perf_counter() - t0
+        done_cells += cells
+        done_sets += len(part)
+        i += chunk
+    return {
+        "value": done_cells / elapsed / 1e9 if elapsed > 0 else None,
+        "unit": "GCUPS",
+        "cores": threads,
+        "kind": "port",
+        "sample": f"first {done_sets} of the {len(sets)} sets ({done_cells / 1e9:.2f} G cells, {elapsed:.1f} s), "
+                  f"8-lane AVX2 i32 kernel, one set per thread",
+    }
+
+
+def load_traffic():
+    """DRAM bytes per launch of the batched kernel from the committed ncu
+    summary, scaled to this run's cells (null when absent)."""
+    path = os.path.join(ROOT, "profiles", "k_batch_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    from minipoa_b200 import workloads
+    from minipoa_b200.params import Params
+
+    params = Params()
+    sets = workloads.batched_sets(args.sets, seed=args.seed + rank)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t_steps = []
+        cb = None
+        for k in range(args.warmup + args.steps):
+            cb = cpu_baseline(sets, params, max(2.0, args.cpu_seconds / max(1, args.steps)))
+            if k >= args.warmup:
+                t_steps.append(cb)
+        vals = [c["value"] for c in t_steps]
+        v = statistics.median(vals)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "sets": args.sets, "seed": args.seed,
+                       "sample": "bounded per step", "l2": "inputs larger than L2"},
+            "cpu_baseline": {**t_steps[-1], "value": v},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import minipoa_b200 as mp
+
+    ctx = mp.Context(local)
+    batch = mp.Batch(params, sets, ctx)
+    for _ in range(args.warmup):
+        batch.run(0)
+    barrier(pg)
+    clocks = ClockSampler(local)
+    clocks.start()
+    steps = []
+    for _ in range(args.steps):
+        steps.append(batch.run(0))
+    clock_info = clocks.stop()
+    barrier(pg)
+    dev_ms = sum(s.device_ms for s in steps)
+    kern_ms = sum(s.kernel_ms for s in steps)
+    cells = sum(s.cells for s in steps)
+    dp_bytes = sum(s.dp_bytes for s in steps)
+    launches = sum(s.launches for s in steps)
+    max_ms = reduce_max(pg, dev_ms)
+    all_cells = reduce_sum(pg, float(cells))
+    value = all_cells / (max_ms / 1e3) / 1e9
+    reads = sum(s.reads for s in steps)
+
+    # end to end through the C ABI from host buffers
+    e2e_vals, h2d, d2h = [], 0, 0
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        b2 = mp.Batch(params, sets, ctx)
+        st = b2.run(0)
+        out = b2.output_all(0)
+        h2d, d2h = b2.transfer_bytes()
+        del b2
+        dt = time.perf_counter() - t0
+        e2e_vals.append(st.cells / dt / 1e9)
+        assert out.count(b">consensus sequence\n") == len(sets)
+    e2e_v = reduce_sum(pg, statistics.median(e2e_vals)) if pg else statistics.median(e2e_vals)
+
+    # plain form (one launch per read) on a prefix of the sets
+    plain = None
+    if args.plain_sets > 0 and rank == 0:
+        sub = sets[: args.plain_sets]
+        bp = mp.Batch(params, sub, ctx)
+        bp.run(0)
+        sb = bp.run(0)
+        sp = bp.run(1)
+        plain = {"sets": len(sub), "plain_gcups": sp.cells / (sp.device_ms / 1e3) / 1e9,
+                 "batched_gcups": sb.cells / (sb.device_ms / 1e3) / 1e9,
+                 "plain_reads_per_s": sp.reads / (sp.device_ms / 1e3),
+                 "batched_reads_per_s": sb.reads / (sb.device_ms / 1e3), "plain_launches": sp.launches}
+        del bp
+
+    peak, peak_kind = measured_peaks()
+    avg_launch_ms = kern_ms / max(1, sum(1 + s.relaunches for s in steps))
+    bytes_per_launch = dp_bytes / max(1, sum(1 + s.relaunches for s in steps))
+    achieved = bytes_per_launch / (avg_launch_ms / 1e3) / 1e9
+    traffic = load_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "algorithmic_bytes": "12 B/cell: the int32 M, D, I states stored per band cell for the traceback",
+                "kernel": "k_batch",
+                "traffic": None if traffic is None else traffic.get("bytes_per_cell", 0) * cells / max(
+                    1, sum(1 + s.relaunches for s in steps))}
+
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline(sets, params, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "sets": args.sets, "seed": args.seed, "reads_per_step": reads // args.steps,
+                       "cells_per_step": cells // args.steps, "l2": "inputs larger than L2 (no flush needed)",
+                       "parallelism": f"{world} independent GPU(s)", "slots": steps[0].slots,
+                       "relaunch_passes": steps[0].relaunches, "reads_per_s": reads / (dev_ms / 1e3)},
+            "roofline": roofline,
+            "cpu_baseline": cb,
+            "e2e": {"value": e2e_v, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+            "plain_vs_batched": plain,
+        }
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,207 @@
+/*
+ * minipoa_b200 -- C ABI of the B200 (sm_100a) partial-order-alignment library.
+ *
+ * Drop-in boundary for minipoa-rs's POA hot path: affine-gap sequence-to-DAG
+ * alignment over toposorted ranks, weighted traceback, read-into-graph fusion
+ * and re-toposort. The DP, traceback, fusion and toposort run on the GPU and
+ * the graph stays resident in device memory between reads; consensus / MSA /
+ * GFA text is rendered on the host from the downloaded graph.
+ *
+ * Each entry point names the reference item it replaces (paths inside the
+ * minipoa-rs project). The reference is a Rust library with no FFI of its
+ * own; INTEGRATION.md shows the extern "C" block a Rust FFI crate binds.
+ *
+ * Conventions: every call returns int status (POA_OK = 0); on failure
+ * poa_last_error(ctx) gives the reference's error text. Buffers passed in are
+ * caller-owned; buffers returned through out-pointers are library-owned and
+ * released with poa_free. No call takes torch or other framework types.
+ */
+#ifndef MINIPOA_B200_H
+#define MINIPOA_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Alignment errors carry the reference's messages
+ * (src/align.rs, src/graph.rs); resource codes are this library's own. */
+enum {
+  POA_OK = 0,
+  POA_ERR_ALIGN = 1,        /* an alignment / graph error (message in poa_last_error) */
+  POA_ERR_INVALID = 2,      /* invalid parameters or arguments (Params::validate text) */
+  POA_ERR_CUDA = 3,         /* CUDA runtime failure, or no CUDA device */
+  POA_ERR_ALLOC = 4,        /* device memory could not be allocated within the budget */
+  POA_ERR_UNSUPPORTED = 5,  /* feature not available in this build (message says which) */
+  POA_ERR_TIMEOUT = 6       /* a bounded device wait gave up */
+};
+
+/* Params (src/lib.rs:47-71). Same field order as the reference struct;
+ * alphabet/matrix point at caller memory (alphabet_len^2 matrix entries). */
+typedef struct poa_params {
+  int32_t match_score;
+  int32_t mismatch;
+  int32_t gap_open;
+  int32_t gap_ext;
+  uint64_t b;
+  uint64_t f;
+  int32_t adaptive;
+  int32_t seeding;
+  uint64_t k;
+  uint64_t w;
+  int32_t progressive;
+  int32_t result;
+  uint64_t threads;
+  uint64_t win_band;
+  uint64_t win_max;
+  double mm_filter_ratio;
+  uint64_t max_occ;
+  uint64_t tr_dist;
+  int32_t verbose;
+  int32_t is_rna;
+  int32_t alphabet_len;
+  int32_t reserved;
+  const uint8_t *alphabet;
+  const int32_t *matrix;
+} poa_params;
+
+/* AlignedBase (src/lib.rs:140-145); -1 encodes None. */
+typedef struct poa_aligned_base {
+  int64_t node;
+  int64_t base;
+  int64_t aligned;
+} poa_aligned_base;
+
+typedef struct poa_ctx poa_ctx;
+typedef struct poa_graph poa_graph;
+typedef struct poa_batch poa_batch;
+
+/* dp_backend() (src/lib.rs:15-37): the DP backend string. */
+const char *poa_dp_backend(void);
+
+/* Context: one CUDA device, one stream, a DP arena and a memory budget in
+ * bytes (0 = 90% of free device memory). No reference counterpart (the
+ * reference keeps a thread-local arena, src/align.rs:222-226). */
+int poa_ctx_create(int device, uint64_t mem_budget, poa_ctx **out);
+void poa_ctx_destroy(poa_ctx *ctx);
+const char *poa_last_error(const poa_ctx *ctx);
+void poa_free(void *ptr);
+
+/* Params::validate (src/lib.rs:149-173). */
+int poa_params_validate(poa_ctx *ctx, const poa_params *params);
+
+/* Graph::new (src/graph.rs:30-40): source and sink nodes, both base N. */
+int poa_graph_new(poa_ctx *ctx, const poa_params *params, poa_graph **out);
+void poa_graph_free(poa_graph *graph);
+
+/* align_sequences (src/lib.rs:177-182): validate, new graph, then the serial
+ * read loop of extend_graph (src/lib.rs:184-204). */
+int poa_align_sequences(poa_ctx *ctx, const poa_params *params, int64_t n_seqs, const uint8_t *const *seqs,
+                        const int64_t *lens, poa_graph **out);
+
+/* extend_graph (src/lib.rs:184-204) on an existing graph, reads
+ * existing..n_seqs-1 (their index is the path's sequence id). */
+int poa_extend_graph(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t n_seqs,
+                     const uint8_t *const *seqs, const int64_t *lens, int64_t existing);
+
+/* align::align (src/align.rs:81-188): the path of `query` against the graph
+ * in its current toposort order, source first, sink excluded. The graph is
+ * not modified. *out has *out_len items; release with poa_free. */
+int poa_align(poa_ctx *ctx, const poa_params *params, poa_graph *graph, const uint8_t *query, int64_t len,
+              poa_aligned_base **out, int64_t *out_len);
+
+/* align::poa (src/align.rs:192-211): align between anchors beg_id (included)
+ * and end_id (excluded) with the full-DP retry. retry = 0 gives poa_inner
+ * (src/align.rs:531-545) without the retry; kernel: 0 = score-guard dispatch
+ * (src/align.rs:493-529), 1 = i32 kernel only, 2 = i64 kernel only. */
+int poa_poa(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t beg_id, int64_t end_id,
+            const uint8_t *query, int64_t len, int32_t adaptive, uint64_t band_b, int32_t kernel, int32_t retry,
+            poa_aligned_base **out, int64_t *out_len);
+
+/* Graph::add_path (src/graph.rs:82-122). */
+int poa_graph_add_path(poa_ctx *ctx, poa_graph *graph, int64_t seq_id, const poa_aligned_base *items, int64_t n);
+/* Graph::add_node (src/graph.rs:42-59) and Graph::add_edge (src/graph.rs:62-79). */
+int poa_graph_add_node(poa_ctx *ctx, poa_graph *graph, int64_t base, int64_t *out_id);
+int poa_graph_add_edge(poa_ctx *ctx, poa_graph *graph, int64_t from, int64_t to);
+/* Graph::toposort (src/graph.rs:125-178); grouped != 0 orders column groups. */
+int poa_graph_toposort(poa_ctx *ctx, poa_graph *graph, int32_t grouped);
+
+/* Graph::consensus (src/graph.rs:181-237): sequence (decoded bytes), node
+ * ids and coverage, each *len long; release each with poa_free. */
+int poa_graph_consensus(poa_ctx *ctx, const poa_params *params, poa_graph *graph, uint8_t **seq, int64_t **ids,
+                        int64_t **coverage, int64_t *len);
+/* Graph::msa (src/graph.rs:239-279): FASTA rows for sequences 0..n-1. */
+int poa_graph_msa(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t n, const char *const *names,
+                  const char *const *comments, char **out, int64_t *out_len);
+/* Graph::gfa (src/graph.rs:281-331). */
+int poa_graph_gfa(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t n, const char *const *names,
+                  char **out, int64_t *out_len);
+
+/* The graph's public fields (src/graph.rs:6-27), downloaded: node count,
+ * path count and sizes of the variable parts. */
+typedef struct poa_graph_sizes {
+  int64_t n_nodes;
+  int64_t n_edges;   /* total incoming entries */
+  int64_t n_paths;
+  int64_t path_items;
+  int64_t alphabet;
+  int64_t n_rank;    /* entries of Graph::rank */
+} poa_graph_sizes;
+int poa_graph_sizes_get(poa_ctx *ctx, poa_graph *graph, poa_graph_sizes *out);
+/* Fills caller buffers (sizes from poa_graph_sizes_get):
+ * fields: 4*n_nodes (base, parent, rank, coverage); rank: n_nodes;
+ * aligned: n_nodes*alphabet (-1 = None); in_cnt/out_cnt: n_nodes;
+ * in_pairs/out_pairs: 2*n_edges (id, weight) in insertion order;
+ * path_seq/path_len: n_paths; path_ids: path_items. */
+int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *rank, int64_t *aligned,
+                     int64_t *in_cnt, int64_t *out_cnt, int64_t *in_pairs, int64_t *out_pairs, int64_t *path_seq,
+                     int64_t *path_len, int64_t *path_ids);
+
+/* ---- batched independent read sets (no reference counterpart: the
+ * reference runs one set per process; each set here is one extend_graph). */
+typedef struct poa_batch_stats {
+  uint64_t cells;       /* 8-aligned band cells computed, retries included */
+  uint64_t reads;       /* reads aligned */
+  double device_ms;     /* device time of the last run (CUDA events) */
+  int32_t launches;     /* kernel launches in the last run */
+  int32_t relaunches;   /* extra passes for jobs that outgrew their DP arena */
+  int32_t slots;        /* concurrent warp slots of the first pass */
+  int32_t reserved;
+  double kernel_ms;     /* device time inside the read-loop kernel launches */
+  uint64_t dp_bytes;    /* DP state bytes stored (M, D, I per cell) */
+} poa_batch_stats;
+
+/* Uploads n_sets read sets (set i = reads set_off[i]..set_off[i+1]-1) and
+ * sizes device storage for them. mode: 0 = persistent batched kernel over all
+ * sets (size-ordered queue), 1 = plain form, one launch per read of each set. */
+int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, const int64_t *set_off,
+                     const uint8_t *const *seqs, const int64_t *lens, poa_batch **out);
+/* Resets every set's graph to Graph::new and aligns all reads on the device.
+ * Inputs already resident; returns after the device work completes. */
+int poa_batch_run(poa_ctx *ctx, poa_batch *batch, int32_t mode, poa_batch_stats *stats);
+/* Per-set status after a run (0 = ok, else POA_ERR_ALIGN with message in
+ * poa_batch_error). */
+int poa_batch_status(poa_ctx *ctx, poa_batch *batch, int64_t set, char **message);
+/* Output of set `set`: result 0 consensus FASTA, 1 MSA, 2 GFA, rendered with
+ * names "read{i}" / empty comments unless names are given. */
+int poa_batch_output(poa_ctx *ctx, poa_batch *batch, int64_t set, int32_t result, const char *const *names,
+                     const char *const *comments, char **out, int64_t *out_len);
+/* Output of every set concatenated in set order (result 0 or 2), rendered
+ * on host threads. */
+int poa_batch_output_all(poa_ctx *ctx, poa_batch *batch, int32_t result, char **out, int64_t *out_len);
+/* One set's graph as a standalone graph handle (copied). */
+int poa_batch_graph(poa_ctx *ctx, poa_batch *batch, int64_t set, poa_graph **out);
+/* Host<->device bytes moved by the last poa_batch_create (reads, offsets,
+ * lengths) and by the last output call (packed graphs). */
+int poa_batch_transfer_bytes(poa_ctx *ctx, poa_batch *batch, uint64_t *h2d, uint64_t *d2h);
+void poa_batch_free(poa_batch *batch);
+
+/* Tuning: concurrent warp slots per SM for the batched kernel (0 = auto) and
+ * the DP arena bytes per slot (0 = auto from the budget). */
+int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1242 @@
+// Host runtime and C ABI of the B200 POA library: CUDA context, growable
+// device-resident graphs, the batched scheduler, and output rendering.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/minipoa_b200.h"
+#include "host_graph.h"
+#include "poa_internal.h"
+#include "poa_pack.h"
+
+using namespace poa;
+
+namespace {
+
+struct CudaError {
+  cudaError_t code;
+  std::string where;
+};
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) throw CudaError{e_, #call};             \
+  } while (0)
+
+struct AlignError {
+  int code;  // POA_ERR_*
+  std::string msg;
+};
+
+std::string status_message(int32_t st, int err_i, int err_j) {
+  switch (st) {
+    case ST_ANCHOR_NOT_IN_GRAPH: return "alignment anchor is not in graph";
+    case ST_ANCHORS_NOT_ORDERED: return "alignment anchors are not topologically ordered";
+    case ST_COORD_LIMITS: return "alignment exceeds coordinate limits";
+    case ST_NO_PATH: return "no graph path connects alignment anchors";
+    case ST_BAND_NO_INTERSECT: return "alignment band does not intersect graph path";
+    case ST_BAND_EXCLUDES_SOURCE: return "alignment band excludes source";
+    case ST_TB_NO_ADVANCE: return "alignment traceback failed to advance";
+    case ST_TB_LEFT_BAND: return "alignment traceback left active band";
+    case ST_TB_NO_PRED:
+      return "alignment traceback has no predecessor at graph row " + std::to_string(err_i) + ", query column " +
+             std::to_string(err_j);
+    case ST_BASE_OUTSIDE: return "alignment base outside alphabet";
+    case ST_UNKNOWN_NODE: return "alignment references an unknown node";
+    case ST_CYCLE: return "graph contains a cycle (possibly between alignment columns)";
+    case ST_COLUMN_DEPS: return "invalid graph column dependencies";
+    case ST_ARENA_FULL: return "DP arena exhausted";
+    case ST_GRAPH_FULL: return "graph capacity exhausted";
+    case ST_SEEDING_UNSUPPORTED: return "seeded windows (-S) are not available in this build";
+    default: return "unknown device status " + std::to_string(st);
+  }
+}
+
+int status_code(int32_t st) {
+  if (is_alignment_error(st)) return POA_ERR_ALIGN;
+  if (st == ST_SEEDING_UNSUPPORTED) return POA_ERR_UNSUPPORTED;
+  return POA_ERR_ALLOC;
+}
+
+struct Caps {
+  int32_t node_cap = 0, chunk_cap = 0, path_cap = 0, max_paths = 0;
+  int sigma = 0;
+};
+
+// Assigns the graph arrays of one job inside `base` (nullptr: size only).
+size_t layout(const Caps &c, char *base, Job *J) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) -> char * {
+    const size_t at = o;
+    o = (o + bytes + 255) / 256 * 256;
+    return base ? base + at : nullptr;
+  };
+  const size_t N = size_t(c.node_cap);
+  J->base = (uint8_t *)take(N);
+  J->parent = (int32_t *)take(N * 4);
+  J->rank = (int32_t *)take(N * 4);
+  J->coverage = (int32_t *)take(N * 4);
+  J->in_head = (int32_t *)take(N * 4);
+  J->in_tail = (int32_t *)take(N * 4);
+  J->in_cnt = (int32_t *)take(N * 4);
+  J->out_head = (int32_t *)take(N * 4);
+  J->out_tail = (int32_t *)take(N * 4);
+  J->out_cnt = (int32_t *)take(N * 4);
+  J->rank_to_node = (int32_t *)take(N * 4);
+  J->aligned = (int32_t *)take(N * size_t(c.sigma) * 4);
+  J->chunk_id = (int32_t *)take(size_t(c.chunk_cap) * CHUNK * 4);
+  J->chunk_w = (int32_t *)take(size_t(c.chunk_cap) * CHUNK * 4);
+  J->chunk_next = (int32_t *)take(size_t(c.chunk_cap) * 4);
+  J->path_items = (int32_t *)take(size_t(c.path_cap) * 4 + 4);
+  J->path_off = (int32_t *)take(size_t(c.max_paths + 1) * 4);
+  J->path_seq = (int32_t *)take(size_t(c.max_paths) * 4 + 4);
+  J->node_cap = c.node_cap;
+  J->chunk_cap = c.chunk_cap;
+  J->path_cap = c.path_cap;
+  J->max_paths = c.max_paths;
+  return o;
+}
+
+// (pointer, bytes) of each array of a laid-out job, in a fixed order.
+std::vector<std::pair<char *, size_t>> arrays(const Job &J, const Caps &c) {
+  const size_t N = size_t(c.node_cap);
+  return {{(char *)J.base, N},
+          {(char *)J.parent, N * 4},
+          {(char *)J.rank, N * 4},
+          {(char *)J.coverage, N * 4},
+          {(char *)J.in_head, N * 4},
+          {(char *)J.in_tail, N * 4},
+          {(char *)J.in_cnt, N * 4},
+          {(char *)J.out_head, N * 4},
+          {(char *)J.out_tail, N * 4},
+          {(char *)J.out_cnt, N * 4},
+          {(char *)J.rank_to_node, N * 4},
+          {(char *)J.aligned, N * size_t(c.sigma) * 4},
+          {(char *)J.chunk_id, size_t(c.chunk_cap) * CHUNK * 4},
+          {(char *)J.chunk_w, size_t(c.chunk_cap) * CHUNK * 4},
+          {(char *)J.chunk_next, size_t(c.chunk_cap) * 4},
+          {(char *)J.path_items, size_t(c.path_cap) * 4 + 4},
+          {(char *)J.path_off, size_t(c.max_paths + 1) * 4},
+          {(char *)J.path_seq, size_t(c.max_paths) * 4 + 4}};
+}
+
+std::vector<uint8_t> encode_table(const HostParams &p) {
+  std::vector<uint8_t> t(256);
+  for (int c = 0; c < 256; ++c) t[size_t(c)] = uint8_t(p.encode(uint8_t(c)));
+  return t;
+}
+
+thread_local std::string g_create_error;
+
+char *dup_string(const std::string &s) {
+  char *o = (char *)std::malloc(s.size() + 1);
+  std::memcpy(o, s.data(), s.size());
+  o[s.size()] = 0;
+  return o;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+struct poa_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;
+  uint64_t allocated = 0;
+  std::string err;
+  char *arena = nullptr;
+  int64_t arena_bytes = 0;
+  uint8_t *qbuf = nullptr;
+  size_t qbuf_bytes = 0;
+  int4 *items = nullptr;
+  int32_t *n_items = nullptr;
+  size_t items_cap = 0;
+  int32_t *d_matrix = nullptr;
+  uint8_t *d_encode = nullptr;
+  size_t matrix_cap = 0;
+
+  void *dalloc(size_t bytes) {
+    if (allocated + bytes > budget) throw AlignError{POA_ERR_ALLOC, "device memory budget exceeded"};
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw AlignError{POA_ERR_ALLOC, std::string("cudaMalloc failed: ") + cudaGetErrorString(e)};
+    }
+    allocated += bytes;
+    return p;
+  }
+  void dfree(void *p, size_t bytes) {
+    if (p) {
+      const cudaError_t e = cudaFree(p);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        std::fprintf(stderr, "minipoa_b200: cudaFree failed: %s\n", cudaGetErrorString(e));
+      }
+      allocated -= std::min<uint64_t>(allocated, bytes);
+    }
+  }
+  void ensure_arena(int64_t bytes) {
+    if (arena_bytes >= bytes) return;
+    dfree(arena, size_t(arena_bytes));
+    arena = nullptr;
+    arena_bytes = 0;
+    arena = (char *)dalloc(size_t(bytes));
+    arena_bytes = bytes;
+  }
+  void ensure_qbuf(size_t bytes) {
+    if (qbuf_bytes >= bytes) return;
+    dfree(qbuf, qbuf_bytes);
+    qbuf = nullptr;
+    qbuf_bytes = 0;
+    qbuf = (uint8_t *)dalloc(bytes);
+    qbuf_bytes = bytes;
+  }
+  void ensure_items(size_t n) {
+    if (items_cap >= n) return;
+    dfree(items, items_cap * sizeof(int4) + 16);
+    items = nullptr;
+    items_cap = 0;
+    char *p = (char *)dalloc(n * sizeof(int4) + 16);
+    items = (int4 *)p;
+    n_items = (int32_t *)(p + n * sizeof(int4));
+    items_cap = n;
+  }
+  DevParams params(const HostParams &hp) {
+    const size_t need = hp.matrix.size();
+    if (matrix_cap < need || !d_matrix) {
+      dfree(d_matrix, matrix_cap * 4);
+      d_matrix = nullptr;
+      d_matrix = (int32_t *)dalloc(std::max<size_t>(need, 1) * 4);
+      matrix_cap = std::max<size_t>(need, 1);
+    }
+    if (!d_encode) d_encode = (uint8_t *)dalloc(256);
+    CK(cudaMemcpyAsync(d_matrix, hp.matrix.data(), need * 4, cudaMemcpyHostToDevice, stream));
+    auto enc = encode_table(hp);
+    CK(cudaMemcpyAsync(d_encode, enc.data(), 256, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    return make_params(hp, d_matrix, d_encode);
+  }
+  static DevParams make_params(const HostParams &hp, const int32_t *m, const uint8_t *e) {
+    DevParams P{};
+    P.matrix = m;
+    P.encode = e;
+    P.sigma = int32_t(hp.alphabet.size());
+    P.unknown = hp.encode('N');
+    P.gap_open_raw = hp.gap_open;
+    P.gap_ext = hp.gap_ext;
+    P.gap_open = hp.gap_open + hp.gap_ext;
+    P.adaptive = hp.adaptive ? 1 : 0;
+    P.kernel = 0;
+    P.seeding = hp.seeding ? 1 : 0;
+    P.b = hp.b;
+    P.f = hp.f;
+    P.largest = hp.largest();
+    return P;
+  }
+};
+
+struct poa_graph {
+  poa_ctx *ctx = nullptr;
+  int sigma = 0, unknown = 0;
+  Caps caps;
+  char *storage = nullptr;
+  size_t bytes = 0;
+  Job *d_job = nullptr;
+  Job h{};
+  int64_t ub_nodes = 0, ub_chunks = 0, ub_path_used = 0, ub_paths = 0;
+
+  ~poa_graph() {
+    if (ctx) {
+      ctx->dfree(storage, bytes);
+      ctx->dfree(d_job, sizeof(Job));
+    }
+  }
+  void sync() {
+    CK(cudaMemcpyAsync(&h, d_job, sizeof(Job), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ub_nodes = h.n_nodes;
+    ub_chunks = h.n_chunks;
+    ub_path_used = h.path_used;
+    ub_paths = h.n_paths;
+  }
+  void upload() {
+    CK(cudaMemcpyAsync(d_job, &h, sizeof(Job), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  // Ensures room for a step that adds at most the given amounts.
+  void reserve(int64_t nodes, int64_t chunks, int64_t path_items, int64_t paths) {
+    if (ub_nodes + nodes <= caps.node_cap && ub_chunks + chunks <= caps.chunk_cap &&
+        ub_path_used + path_items <= caps.path_cap && ub_paths + paths <= caps.max_paths) {
+      ub_nodes += nodes;
+      ub_chunks += chunks;
+      ub_path_used += path_items;
+      ub_paths += paths;
+      return;
+    }
+    sync();
+    Caps nc = caps;
+    auto grow = [](int32_t cap, int64_t need) {
+      int64_t c = cap;
+      while (c < need) c = std::max<int64_t>(c * 2, 64);
+      if (c > INT32_MAX / 2) c = INT32_MAX / 2;
+      return int32_t(c);
+    };
+    nc.node_cap = grow(caps.node_cap, ub_nodes + nodes);
+    nc.chunk_cap = grow(caps.chunk_cap, ub_chunks + chunks);
+    nc.path_cap = grow(caps.path_cap, ub_path_used + path_items);
+    nc.max_paths = grow(caps.max_paths, ub_paths + paths);
+    if (nc.node_cap != caps.node_cap || nc.chunk_cap != caps.chunk_cap || nc.path_cap != caps.path_cap ||
+        nc.max_paths != caps.max_paths) {
+      Job nj = h;
+      const size_t nbytes = layout(nc, nullptr, &nj);
+      char *ns = (char *)ctx->dalloc(nbytes);
+      layout(nc, ns, &nj);
+      auto olda = arrays(h, caps);
+      auto newa = arrays(nj, nc);
+      for (size_t k = 0; k < olda.size(); ++k)
+        CK(cudaMemcpyAsync(newa[k].first, olda[k].first, olda[k].second, cudaMemcpyDeviceToDevice, ctx->stream));
+      nj.n_nodes = h.n_nodes;
+      CK(cudaStreamSynchronize(ctx->stream));
+      ctx->dfree(storage, bytes);
+      storage = ns;
+      bytes = nbytes;
+      caps = nc;
+      h = nj;
+      upload();
+    }
+    ub_nodes += nodes;
+    ub_chunks += chunks;
+    ub_path_used += path_items;
+    ub_paths += paths;
+  }
+  void check_status() {
+    sync();
+    if (h.status != ST_OK) {
+      const int32_t st = h.status;
+      h.status = ST_OK;
+      upload();
+      throw AlignError{status_code(st), status_message(st, h.err_i, h.err_j)};
+    }
+  }
+  HostGraph download() {
+    sync();
+    const int64_t words = packed_words(h, sigma);
+    int32_t *d_out = (int32_t *)ctx->dalloc(size_t(words) * 4 + 16);
+    int64_t *d_off = (int64_t *)ctx->dalloc(16);
+    int32_t *d_id = (int32_t *)ctx->dalloc(16);
+    std::vector<int32_t> rec(static_cast<size_t>(words));
+    try {
+      const int64_t zero = 0;
+      const int32_t zid = 0;
+      CK(cudaMemcpyAsync(d_off, &zero, 8, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(d_id, &zid, 4, cudaMemcpyHostToDevice, ctx->stream));
+      CK(launch_pack(d_job, d_id, 1, d_off, d_out, sigma, ctx->stream));
+      CK(cudaMemcpyAsync(rec.data(), d_out, size_t(words) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+    } catch (...) {
+      ctx->dfree(d_out, size_t(words) * 4 + 16);
+      ctx->dfree(d_off, 16);
+      ctx->dfree(d_id, 16);
+      throw;
+    }
+    ctx->dfree(d_out, size_t(words) * 4 + 16);
+    ctx->dfree(d_off, 16);
+    ctx->dfree(d_id, 16);
+    return HostGraph::parse(rec.data());
+  }
+};
+
+namespace {
+
+poa_graph *new_graph(poa_ctx *ctx, const HostParams &hp, Caps caps) {
+  auto g = std::make_unique<poa_graph>();
+  g->ctx = ctx;
+  g->sigma = int(hp.alphabet.size());
+  g->unknown = hp.encode('N');
+  caps.sigma = g->sigma;
+  caps.node_cap = std::max(caps.node_cap, 64);
+  caps.chunk_cap = std::max(caps.chunk_cap, 64);
+  caps.path_cap = std::max(caps.path_cap, 64);
+  caps.max_paths = std::max(caps.max_paths, 8);
+  g->caps = caps;
+  Job J{};
+  g->bytes = layout(caps, nullptr, &J);
+  g->storage = (char *)ctx->dalloc(g->bytes);
+  layout(caps, g->storage, &J);
+  g->d_job = (Job *)ctx->dalloc(sizeof(Job));
+  g->h = J;
+  g->upload();
+  CK(launch_reset(g->d_job, 1, g->sigma, g->unknown, ctx->stream));
+  g->sync();
+  return g.release();
+}
+
+template <class F>
+int api(poa_ctx *ctx, F &&f) {
+  try {
+    f();
+    if (ctx) ctx->err.clear();
+    return POA_OK;
+  } catch (const AlignError &e) {
+    if (ctx) ctx->err = e.msg;
+    return e.code;
+  } catch (const CudaError &e) {
+    if (ctx) ctx->err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    return POA_ERR_CUDA;
+  } catch (const std::bad_alloc &) {
+    if (ctx) ctx->err = "host allocation failed";
+    return POA_ERR_ALLOC;
+  }
+}
+
+HostParams checked_params(const poa_params *p) {
+  if (!p) throw AlignError{POA_ERR_INVALID, "null params"};
+  HostParams hp = HostParams::from(p);
+  std::string v = hp.validate();
+  if (!v.empty()) throw AlignError{POA_ERR_INVALID, v};
+  return hp;
+}
+
+// Runs the single-graph read loop reads[r0..r1) with arena growth on demand.
+void extend_range(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::vector<const uint8_t *> &seqs,
+                  const std::vector<int64_t> &lens, int64_t r0) {
+  if (hp.progressive && r0 == 0) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
+  const int64_t n = int64_t(seqs.size());
+  if (r0 >= n) return;
+  int64_t total = 0, maxlen = 0;
+  for (int64_t r = r0; r < n; ++r) {
+    if (lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+    total += lens[r];
+    maxlen = std::max(maxlen, lens[r]);
+  }
+  g->reserve(total + 2 * (n - r0), 2 * (total + 3 * (n - r0)), total + (n - r0), n - r0);
+  DevParams P = ctx->params(hp);
+  // reads, offsets and lengths in one upload
+  const size_t off_bytes = size_t(n) * 8, len_bytes = size_t(n) * 4;
+  const size_t need = off_bytes + len_bytes + size_t(std::max<int64_t>(total, 1)) + 64;
+  ctx->ensure_qbuf(need);
+  std::vector<uint8_t> host(need);
+  int64_t *off = (int64_t *)host.data();
+  int32_t *ln = (int32_t *)(host.data() + off_bytes);
+  uint8_t *rd = host.data() + off_bytes + len_bytes;
+  int64_t at = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    off[r] = at;
+    ln[r] = int32_t(r >= r0 ? lens[r] : 0);
+    if (r >= r0 && lens[r] > 0) std::memcpy(rd + at, seqs[r], size_t(lens[r]));
+    if (r >= r0) at += lens[r];
+  }
+  CK(cudaMemcpyAsync(ctx->qbuf, host.data(), need, cudaMemcpyHostToDevice, ctx->stream));
+  const int64_t *d_off = (const int64_t *)ctx->qbuf;
+  const int32_t *d_len = (const int32_t *)(ctx->qbuf + off_bytes);
+  const uint8_t *d_rd = ctx->qbuf + off_bytes + len_bytes;
+  // the device advances next_read after each completed read
+  g->sync();
+  g->h.next_read = int32_t(r0);
+  g->h.status = ST_OK;
+  g->upload();
+  // initial arena: scratch + a static-band estimate, grown on ARENA_FULL
+  int64_t arena = std::max<int64_t>(int64_t(64) << 20, ctx->arena_bytes);
+  int64_t r = r0;
+  for (;;) {
+    ctx->ensure_arena(arena);
+    CK(launch_extend_range(g->d_job, P, ctx->arena, ctx->arena_bytes, d_rd, d_off, d_len, int(r), int(n),
+                           ctx->stream));
+    g->sync();
+    if (g->h.status == ST_OK) break;
+    const int32_t st = g->h.status;
+    if (st == ST_ARENA_FULL) {
+      r = g->h.next_read;
+      g->h.status = ST_OK;
+      g->upload();
+      if (arena >= int64_t(ctx->budget)) throw AlignError{POA_ERR_ALLOC, "DP arena exceeds the memory budget"};
+      arena = std::min<int64_t>(arena * 2, int64_t(ctx->budget - std::min(ctx->budget, ctx->allocated)) +
+                                               ctx->arena_bytes);
+      continue;
+    }
+    g->h.status = ST_OK;
+    g->upload();
+    throw AlignError{status_code(st), status_message(st, g->h.err_i, g->h.err_j)};
+  }
+}
+
+// align / poa on a graph without changing it.
+std::vector<poa_aligned_base> align_path(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const uint8_t *q,
+                                         int64_t len, int mode, int64_t beg, int64_t end, int adaptive,
+                                         uint64_t band_b, int kernel, int retry) {
+  if (len < 0 || len > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+  if (mode == 0 && hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
+  DevParams P = ctx->params(hp);
+  P.kernel = kernel;
+  ctx->ensure_qbuf(size_t(len) + 16);
+  if (len) CK(cudaMemcpyAsync(ctx->qbuf, q, size_t(len), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->ensure_items(size_t(len) + 4);
+  g->sync();
+  if (beg < 0 || end < 0 || beg >= g->h.n_nodes || end >= g->h.n_nodes) {
+    if (mode == 1) throw AlignError{POA_ERR_ALIGN, "alignment anchor is not in graph"};
+  }
+  int64_t arena = std::max<int64_t>(int64_t(64) << 20, ctx->arena_bytes);
+  for (;;) {
+    ctx->ensure_arena(arena);
+    CK(launch_align(g->d_job, P, ctx->arena, ctx->arena_bytes, ctx->qbuf, int(len), mode, int(beg), int(end),
+                    adaptive, band_b, retry, ctx->items, ctx->n_items, ctx->stream));
+    g->sync();
+    const int32_t st = g->h.status;
+    if (st == ST_OK) break;
+    g->h.status = ST_OK;
+    g->upload();
+    if (st == ST_ARENA_FULL) {
+      if (arena >= int64_t(ctx->budget)) throw AlignError{POA_ERR_ALLOC, "DP arena exceeds the memory budget"};
+      arena *= 2;
+      continue;
+    }
+    throw AlignError{status_code(st), status_message(st, g->h.err_i, g->h.err_j)};
+  }
+  int32_t n = 0;
+  CK(cudaMemcpyAsync(&n, ctx->n_items, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<int4> it(size_t(std::max(n, 0)));
+  if (n > 0) CK(cudaMemcpyAsync(it.data(), ctx->items, size_t(n) * sizeof(int4), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<poa_aligned_base> out(it.size());
+  for (size_t k = 0; k < it.size(); ++k) out[k] = {it[k].x, it[k].y, it[k].z};
+  return out;
+}
+
+std::vector<std::string> name_list(int64_t n, const char *const *names, const char *prefix) {
+  std::vector<std::string> v(size_t(std::max<int64_t>(n, 0)));
+  for (int64_t i = 0; i < n; ++i) v[size_t(i)] = names ? std::string(names[i]) : std::string(prefix) + std::to_string(i);
+  return v;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Batch of independent read sets.
+
+struct poa_batch {
+  poa_ctx *ctx = nullptr;
+  HostParams hp;
+  DevParams P{};
+  int64_t n_sets = 0;
+  std::vector<int64_t> set_off;
+  std::vector<int64_t> lens;
+  int sigma = 0, unknown = 0;
+  uint8_t *d_reads = nullptr;
+  int64_t *d_read_off = nullptr;
+  int32_t *d_read_len = nullptr;
+  size_t reads_bytes = 0;
+  int32_t *d_matrix = nullptr;
+  uint8_t *d_encode = nullptr;
+  char *storage = nullptr;
+  size_t storage_bytes = 0;
+  std::vector<Job> jobs;
+  std::vector<Caps> caps;
+  Job *d_jobs = nullptr;
+  std::vector<int32_t> order;
+  int32_t *d_order = nullptr;
+  int32_t *d_queue = nullptr;
+  char *arenas = nullptr;
+  int64_t arena_pool = 0;
+  int warps_per_sm = 0;
+  uint64_t slot_bytes_override = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, k0 = nullptr, k1 = nullptr;
+  bool ran = false;
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;
+
+  ~poa_batch() {
+    if (!ctx) return;
+    ctx->dfree(d_read_off, reads_bytes);  // base of the reads allocation
+    ctx->dfree(d_matrix, 0);
+    ctx->dfree(d_encode, 0);
+    ctx->dfree(storage, storage_bytes);
+    ctx->dfree(d_jobs, jobs.size() * sizeof(Job));
+    ctx->dfree(d_order, order.size() * 4 + 4);
+    ctx->dfree(d_queue, 16);
+    ctx->dfree(arenas, size_t(arena_pool));
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (k0) cudaEventDestroy(k0);
+    if (k1) cudaEventDestroy(k1);
+  }
+
+  void download_jobs() {
+    CK(cudaMemcpyAsync(jobs.data(), d_jobs, jobs.size() * sizeof(Job), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  void upload_jobs() {
+    CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, ctx->stream));
+  }
+
+  // Packs the graphs of `ids` and parses them on the host.
+  std::vector<HostGraph> graphs(const std::vector<int32_t> &ids) {
+    download_jobs();
+    std::vector<int64_t> off(ids.size() + 1, 0);
+    for (size_t k = 0; k < ids.size(); ++k) off[k + 1] = off[k] + packed_words(jobs[size_t(ids[k])], sigma);
+    const size_t words = size_t(off.back());
+    int32_t *d_out = (int32_t *)ctx->dalloc(words * 4 + 16);
+    int64_t *d_off = (int64_t *)ctx->dalloc(off.size() * 8);
+    int32_t *d_ids = (int32_t *)ctx->dalloc(ids.size() * 4 + 4);
+    std::vector<int32_t> rec(words + 1);
+    auto release = [&] {
+      ctx->dfree(d_out, words * 4 + 16);
+      ctx->dfree(d_off, off.size() * 8);
+      ctx->dfree(d_ids, ids.size() * 4 + 4);
+    };
+    try {
+      CK(cudaMemcpyAsync(d_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+      CK(launch_pack(d_jobs, d_ids, int(ids.size()), d_off, d_out, sigma, ctx->stream));
+      CK(cudaMemcpyAsync(rec.data(), d_out, words * 4, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      d2h_bytes = words * 4 + jobs.size() * sizeof(Job);
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+    std::vector<HostGraph> out(ids.size());
+    const int nt = std::max(1, std::min<int>(int(std::thread::hardware_concurrency()), 32));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+      pool.emplace_back([&, t] {
+        for (size_t k = size_t(t); k < ids.size(); k += size_t(nt)) out[k] = HostGraph::parse(rec.data() + off[k]);
+      });
+    for (auto &th : pool) th.join();
+    return out;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+const char *poa_dp_backend(void) { return "cuda-sm100a (warp-per-job, i32 / guarded i64)"; }
+
+int poa_ctx_create(int device, uint64_t mem_budget, poa_ctx **out) {
+  *out = nullptr;
+  auto ctx = std::make_unique<poa_ctx>();
+  int rc = api(ctx.get(), [&] {
+    int count = 0;
+    CK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw AlignError{POA_ERR_CUDA, "no such CUDA device"};
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) throw AlignError{POA_ERR_CUDA, "this build targets sm_100a (B200)"};
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    ctx->budget = mem_budget ? std::min<uint64_t>(mem_budget, free_b) : uint64_t(double(free_b) * 0.9);
+  });
+  if (rc != POA_OK) {
+    g_create_error = ctx->err;
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    return rc;
+  }
+  *out = ctx.release();
+  return POA_OK;
+}
+
+void poa_ctx_destroy(poa_ctx *ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->dfree(ctx->arena, size_t(ctx->arena_bytes));
+  ctx->dfree(ctx->qbuf, ctx->qbuf_bytes);
+  ctx->dfree(ctx->items, 0);
+  ctx->dfree(ctx->d_matrix, 0);
+  ctx->dfree(ctx->d_encode, 0);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+// With a null context: the error of the last failed poa_ctx_create.
+const char *poa_last_error(const poa_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+void poa_free(void *ptr) { std::free(ptr); }
+
+int poa_params_validate(poa_ctx *ctx, const poa_params *params) {
+  return api(ctx, [&] { checked_params(params); });
+}
+
+int poa_graph_new(poa_ctx *ctx, const poa_params *params, poa_graph **out) {
+  *out = nullptr;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    *out = new_graph(ctx, hp, Caps{});
+  });
+}
+
+void poa_graph_free(poa_graph *graph) { delete graph; }
+
+int poa_align_sequences(poa_ctx *ctx, const poa_params *params, int64_t n_seqs, const uint8_t *const *seqs,
+                        const int64_t *lens, poa_graph **out) {
+  *out = nullptr;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    int64_t total = 0;
+    for (int64_t r = 0; r < n_seqs; ++r) total += lens[r];
+    Caps c;
+    c.node_cap = int32_t(std::min<int64_t>(total + 2 * n_seqs + 4, INT32_MAX / 2));
+    c.chunk_cap = int32_t(std::min<int64_t>(2 * (total + 3 * n_seqs) + 8, INT32_MAX / 2));
+    c.path_cap = int32_t(std::min<int64_t>(total + n_seqs + 1, INT32_MAX / 2));
+    c.max_paths = int32_t(n_seqs + 1);
+    std::unique_ptr<poa_graph> g(new_graph(ctx, hp, c));
+    std::vector<const uint8_t *> s(seqs, seqs + n_seqs);
+    std::vector<int64_t> l(lens, lens + n_seqs);
+    extend_range(ctx, hp, g.get(), s, l, 0);
+    *out = g.release();
+  });
+}
+
+int poa_extend_graph(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t n_seqs,
+                     const uint8_t *const *seqs, const int64_t *lens, int64_t existing) {
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    HostParams ap = hp;
+    if (existing > 0) ap.progressive = false;
+    std::vector<const uint8_t *> s(seqs, seqs + n_seqs);
+    std::vector<int64_t> l(lens, lens + n_seqs);
+    extend_range(ctx, ap, graph, s, l, existing);
+  });
+}
+
+int poa_align(poa_ctx *ctx, const poa_params *params, poa_graph *graph, const uint8_t *query, int64_t len,
+              poa_aligned_base **out, int64_t *out_len) {
+  *out = nullptr;
+  *out_len = 0;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    auto v = align_path(ctx, hp, graph, query, len, 0, 0, 1, 0, hp.b, 0, 1);
+    *out = (poa_aligned_base *)std::malloc(sizeof(poa_aligned_base) * (v.size() + 1));
+    std::memcpy(*out, v.data(), v.size() * sizeof(poa_aligned_base));
+    *out_len = int64_t(v.size());
+  });
+}
+
+int poa_poa(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t beg_id, int64_t end_id,
+            const uint8_t *query, int64_t len, int32_t adaptive, uint64_t band_b, int32_t kernel, int32_t retry,
+            poa_aligned_base **out, int64_t *out_len) {
+  *out = nullptr;
+  *out_len = 0;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    if (kernel < 0 || kernel > 2) throw AlignError{POA_ERR_INVALID, "kernel must be 0, 1 or 2"};
+    auto v = align_path(ctx, hp, graph, query, len, 1, beg_id, end_id, adaptive, band_b, kernel, retry);
+    *out = (poa_aligned_base *)std::malloc(sizeof(poa_aligned_base) * (v.size() + 1));
+    std::memcpy(*out, v.data(), v.size() * sizeof(poa_aligned_base));
+    *out_len = int64_t(v.size());
+  });
+}
+
+int poa_graph_add_path(poa_ctx *ctx, poa_graph *graph, int64_t seq_id, const poa_aligned_base *items, int64_t n) {
+  return api(ctx, [&] {
+    if (n < 0 || n > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "alignment is too long"};
+    std::vector<int4> it(static_cast<size_t>(n));
+    for (int64_t k = 0; k < n; ++k) {
+      auto clamp = [](int64_t v) { return int32_t(v < -1 ? INT32_MAX : (v > INT32_MAX ? INT32_MAX : v)); };
+      it[size_t(k)] = make_int4(clamp(items[k].node), items[k].base < 0 ? -1 : clamp(items[k].base),
+                                clamp(items[k].aligned), 0);
+    }
+    graph->reserve(n, 2 * (n + 1), n, 1);
+    ctx->ensure_items(size_t(n) + 4);
+    if (n) CK(cudaMemcpyAsync(ctx->items, it.data(), size_t(n) * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+    DevParams P{};
+    P.sigma = graph->sigma;
+    CK(launch_add_path(graph->d_job, P, int(seq_id), ctx->items, int(n), ctx->stream));
+    graph->check_status();
+  });
+}
+
+int poa_graph_add_node(poa_ctx *ctx, poa_graph *graph, int64_t base, int64_t *out_id) {
+  return api(ctx, [&] {
+    if (base < 0 || base >= graph->sigma) throw AlignError{POA_ERR_INVALID, "alignment base outside alphabet"};
+    graph->reserve(1, 0, 0, 0);
+    CK(launch_add_node(graph->d_job, graph->sigma, int(base), ctx->stream));
+    graph->check_status();
+    *out_id = graph->h.err_i;
+  });
+}
+
+int poa_graph_add_edge(poa_ctx *ctx, poa_graph *graph, int64_t from, int64_t to) {
+  return api(ctx, [&] {
+    graph->sync();
+    if (from < 0 || to < 0 || from >= graph->h.n_nodes || to >= graph->h.n_nodes)
+      throw AlignError{POA_ERR_INVALID, "edge references an unknown node"};
+    graph->reserve(0, 2, 0, 0);
+    CK(launch_add_edge(graph->d_job, int(from), int(to), ctx->stream));
+    graph->check_status();
+  });
+}
+
+int poa_graph_toposort(poa_ctx *ctx, poa_graph *graph, int32_t grouped) {
+  return api(ctx, [&] {
+    if (grouped) {
+      // Column-grouped ranks are computed on the host graph and written back.
+      HostGraph hg = graph->download();
+      std::vector<int32_t> node_rank, order;
+      std::string err;
+      if (!hg.grouped_ranks(node_rank, order, err)) throw AlignError{POA_ERR_ALIGN, err};
+      if (!node_rank.empty())
+        CK(cudaMemcpyAsync(graph->h.rank, node_rank.data(), node_rank.size() * 4, cudaMemcpyHostToDevice,
+                           ctx->stream));
+      if (!order.empty())
+        CK(cudaMemcpyAsync(graph->h.rank_to_node, order.data(), order.size() * 4, cudaMemcpyHostToDevice,
+                           ctx->stream));
+      graph->h.n_rank = int32_t(order.size());
+      graph->upload();
+      return;
+    }
+    graph->sync();
+    ctx->ensure_arena(std::max<int64_t>(int64_t(graph->h.n_nodes) * 8 + 64, int64_t(1) << 20));
+    CK(launch_toposort(graph->d_job, ctx->arena, ctx->arena_bytes, ctx->stream));
+    graph->check_status();
+  });
+}
+
+int poa_graph_consensus(poa_ctx *ctx, const poa_params *params, poa_graph *graph, uint8_t **seq, int64_t **ids,
+                        int64_t **coverage, int64_t *len) {
+  *seq = nullptr;
+  *ids = *coverage = nullptr;
+  *len = 0;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    HostGraph hg = graph->download();
+    std::vector<uint8_t> s;
+    std::vector<int64_t> id, cv;
+    hg.consensus(hp, s, id, cv);
+    *seq = (uint8_t *)std::malloc(s.size() + 1);
+    std::memcpy(*seq, s.data(), s.size());
+    (*seq)[s.size()] = 0;
+    *ids = (int64_t *)std::malloc(id.size() * 8 + 8);
+    *coverage = (int64_t *)std::malloc(cv.size() * 8 + 8);
+    std::memcpy(*ids, id.data(), id.size() * 8);
+    std::memcpy(*coverage, cv.data(), cv.size() * 8);
+    *len = int64_t(s.size());
+  });
+}
+
+int poa_graph_msa(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t n, const char *const *names,
+                  const char *const *comments, char **out, int64_t *out_len) {
+  *out = nullptr;
+  *out_len = 0;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    HostGraph hg = graph->download();
+    auto nm = name_list(n, names, "read");
+    std::vector<std::string> cm(size_t(std::max<int64_t>(n, 0)));
+    for (int64_t i = 0; i < n && comments; ++i) cm[size_t(i)] = comments[i];
+    std::string s, err;
+    if (!hg.msa(hp, nm, cm, s, err)) throw AlignError{POA_ERR_ALIGN, err};
+    *out = dup_string(s);
+    *out_len = int64_t(s.size());
+  });
+}
+
+int poa_graph_gfa(poa_ctx *ctx, const poa_params *params, poa_graph *graph, int64_t n, const char *const *names,
+                  char **out, int64_t *out_len) {
+  *out = nullptr;
+  *out_len = 0;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    HostGraph hg = graph->download();
+    auto nm = name_list(n, names, "read");
+    std::string s, err;
+    if (!hg.gfa(hp, nm, s, err)) throw AlignError{POA_ERR_ALIGN, err};
+    *out = dup_string(s);
+    *out_len = int64_t(s.size());
+  });
+}
+
+int poa_graph_sizes_get(poa_ctx *ctx, poa_graph *graph, poa_graph_sizes *out) {
+  return api(ctx, [&] {
+    graph->sync();
+    out->n_nodes = graph->h.n_nodes;
+    out->n_edges = graph->h.n_edges;
+    out->n_paths = graph->h.n_paths;
+    out->path_items = graph->h.path_used;
+    out->alphabet = graph->sigma;
+    out->n_rank = graph->h.n_rank;
+  });
+}
+
+int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *rank, int64_t *aligned,
+                     int64_t *in_cnt, int64_t *out_cnt, int64_t *in_pairs, int64_t *out_pairs, int64_t *path_seq,
+                     int64_t *path_len, int64_t *path_ids) {
+  return api(ctx, [&] {
+    HostGraph g = graph->download();
+    for (int i = 0; i < g.n; ++i) {
+      fields[4 * i] = g.base[i];
+      fields[4 * i + 1] = g.parent[i];
+      fields[4 * i + 2] = g.rank[i];
+      fields[4 * i + 3] = g.coverage[i];
+      in_cnt[i] = g.in_off[i + 1] - g.in_off[i];
+      out_cnt[i] = g.out_off[i + 1] - g.out_off[i];
+    }
+    for (int i = 0; i < g.n_rank; ++i) rank[i] = g.rank_to_node[i];
+    for (int64_t k = 0; k < int64_t(g.aligned.size()); ++k) aligned[k] = g.aligned[size_t(k)];
+    for (size_t k = 0; k < g.in_id.size(); ++k) {
+      in_pairs[2 * k] = g.in_id[k];
+      in_pairs[2 * k + 1] = g.in_w[k];
+    }
+    for (size_t k = 0; k < g.out_id.size(); ++k) {
+      out_pairs[2 * k] = g.out_id[k];
+      out_pairs[2 * k + 1] = g.out_w[k];
+    }
+    for (size_t p = 0; p < g.path_seq.size(); ++p) {
+      path_seq[p] = g.path_seq[p];
+      path_len[p] = g.path_off[p + 1] - g.path_off[p];
+    }
+    for (size_t k = 0; k < g.path_items.size(); ++k) path_ids[k] = g.path_items[k];
+  });
+}
+
+// ---- batch
+
+int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, const int64_t *set_off,
+                     const uint8_t *const *seqs, const int64_t *lens, poa_batch **out) {
+  *out = nullptr;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    if (hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
+    if (hp.progressive) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
+    auto b = std::make_unique<poa_batch>();
+    b->ctx = ctx;
+    b->hp = hp;
+    b->n_sets = n_sets;
+    b->set_off.assign(set_off, set_off + n_sets + 1);
+    const int64_t n_reads = set_off[n_sets];
+    b->lens.assign(lens, lens + n_reads);
+    b->sigma = int(hp.alphabet.size());
+    b->unknown = hp.encode('N');
+    // reads: offsets, lengths, bytes
+    int64_t total = 0;
+    for (int64_t r = 0; r < n_reads; ++r) {
+      if (lens[r] < 0 || lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+      total += lens[r];
+    }
+    const size_t off_bytes = size_t(n_reads) * 8 + 8, len_bytes = size_t(n_reads) * 4 + 4;
+    b->reads_bytes = off_bytes + len_bytes + size_t(total) + 64;
+    char *rb = (char *)ctx->dalloc(b->reads_bytes);
+    b->d_read_off = (int64_t *)rb;
+    b->d_read_len = (int32_t *)(rb + off_bytes);
+    b->d_reads = (uint8_t *)(rb + off_bytes + len_bytes);
+    {
+      std::vector<char> host(b->reads_bytes);
+      int64_t *off = (int64_t *)host.data();
+      int32_t *ln = (int32_t *)(host.data() + off_bytes);
+      char *rd = host.data() + off_bytes + len_bytes;
+      int64_t at = 0;
+      for (int64_t r = 0; r < n_reads; ++r) {
+        off[r] = at;
+        ln[r] = int32_t(lens[r]);
+        if (lens[r]) std::memcpy(rd + at, seqs[r], size_t(lens[r]));
+        at += lens[r];
+      }
+      CK(cudaMemcpyAsync(rb, host.data(), b->reads_bytes, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      b->h2d_bytes = b->reads_bytes;
+    }
+    b->d_matrix = (int32_t *)ctx->dalloc(hp.matrix.size() * 4 + 4);
+    b->d_encode = (uint8_t *)ctx->dalloc(256);
+    CK(cudaMemcpyAsync(b->d_matrix, hp.matrix.data(), hp.matrix.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    auto enc = encode_table(hp);
+    CK(cudaMemcpyAsync(b->d_encode, enc.data(), 256, cudaMemcpyHostToDevice, ctx->stream));
+    b->P = poa_ctx::make_params(hp, b->d_matrix, b->d_encode);
+    // graph storage: exact worst case of each set
+    b->jobs.resize(size_t(n_sets));
+    b->caps.resize(size_t(n_sets));
+    std::vector<size_t> at(size_t(n_sets) + 1, 0);
+    for (int64_t s = 0; s < n_sets; ++s) {
+      int64_t sum = 0;
+      const int64_t k = set_off[s + 1] - set_off[s];
+      for (int64_t r = set_off[s]; r < set_off[s + 1]; ++r) sum += lens[r];
+      Caps c;
+      c.sigma = b->sigma;
+      c.node_cap = int32_t(std::min<int64_t>(sum + 2 * k + 8, INT32_MAX / 2));
+      c.chunk_cap = int32_t(std::min<int64_t>(2 * (sum + 3 * k) + 16, INT32_MAX / 2));
+      c.path_cap = int32_t(std::min<int64_t>(sum + k + 1, INT32_MAX / 2));
+      c.max_paths = int32_t(k + 1);
+      b->caps[size_t(s)] = c;
+      Job J{};
+      at[size_t(s) + 1] = at[size_t(s)] + layout(c, nullptr, &J);
+    }
+    b->storage_bytes = at.back();
+    b->storage = (char *)ctx->dalloc(b->storage_bytes);
+    for (int64_t s = 0; s < n_sets; ++s) {
+      Job &J = b->jobs[size_t(s)];
+      J = Job{};
+      layout(b->caps[size_t(s)], b->storage + at[size_t(s)], &J);
+      J.reads = b->d_reads;
+      J.read_off = b->d_read_off + set_off[s];
+      J.read_len = b->d_read_len + set_off[s];
+      J.n_reads = int32_t(set_off[s + 1] - set_off[s]);
+    }
+    b->d_jobs = (Job *)ctx->dalloc(b->jobs.size() * sizeof(Job) + 16);
+    b->upload_jobs();
+    // size-ordered queue: largest estimated work first
+    std::vector<double> est(size_t(n_sets), 0.0);
+    for (int64_t s = 0; s < n_sets; ++s) {
+      double mx = 0, sum = 0;
+      for (int64_t r = set_off[s]; r < set_off[s + 1]; ++r) {
+        mx = std::max(mx, double(lens[r]));
+        sum += double(lens[r]);
+      }
+      const double w = 2.0 * (double(hp.b) + (hp.f ? mx / double(hp.f) : mx)) + 16.0;
+      est[size_t(s)] = sum * std::min(w, mx + 16.0);
+    }
+    b->order.resize(size_t(n_sets));
+    std::iota(b->order.begin(), b->order.end(), 0);
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return est[a] > est[c]; });
+    b->d_order = (int32_t *)ctx->dalloc(b->order.size() * 4 + 4);
+    b->d_queue = (int32_t *)ctx->dalloc(16);
+    CK(cudaEventCreate(&b->e0));
+    CK(cudaEventCreate(&b->e1));
+    CK(cudaEventCreate(&b->k0));
+    CK(cudaEventCreate(&b->k1));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = b.release();
+  });
+}
+
+int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot) {
+  return api(ctx, [&] {
+    batch->warps_per_sm = warps_per_sm;
+    batch->slot_bytes_override = arena_bytes_per_slot;
+  });
+}
+
+int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *stats) {
+  return api(ctx, [&] {
+    if (mode != 0 && mode != 1) throw AlignError{POA_ERR_INVALID, "mode must be 0 (batched) or 1 (plain)"};
+    // arena pool: the rest of the budget, allocated once
+    if (!b->arenas) {
+      const uint64_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
+      const int64_t pool = int64_t(left) - (int64_t(256) << 20);
+      if (pool < (int64_t(64) << 20)) throw AlignError{POA_ERR_ALLOC, "no device memory left for DP arenas"};
+      b->arenas = (char *)ctx->dalloc(size_t(pool));
+      b->arena_pool = pool;
+    }
+    const int sms = ctx->sm_count;
+    int wps = b->warps_per_sm > 0 ? b->warps_per_sm : 16;
+    int passes = 0, launches = 0;
+    double kernel_ms = 0;
+    CK(cudaEventRecord(b->e0, ctx->stream));
+    CK(launch_reset(b->d_jobs, int(b->n_sets), b->sigma, b->unknown, ctx->stream));
+    ++launches;
+    int slots_first = 0;
+    if (mode == 0) {
+      std::vector<int32_t> pending = b->order;
+      int64_t slots = int64_t(sms) * wps;
+      for (;;) {
+        slots = std::max<int64_t>(1, std::min<int64_t>(slots, int64_t(pending.size())));
+        int64_t slot_bytes = b->arena_pool / slots / 256 * 256;
+        if (b->slot_bytes_override && passes == 0)
+          slot_bytes = std::min<int64_t>(int64_t(b->slot_bytes_override), slot_bytes);
+        if (passes == 0) slots_first = int(slots);
+        CK(cudaMemcpyAsync(b->d_order, pending.data(), pending.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(b->d_queue, 0, 4, ctx->stream));
+        CK(cudaEventRecord(b->k0, ctx->stream));
+        CK(launch_batch(b->d_jobs, b->d_order, int(pending.size()), b->d_queue, b->P, b->arenas, slot_bytes,
+                        int(slots), ctx->stream));
+        CK(cudaEventRecord(b->k1, ctx->stream));
+        ++launches;
+        ++passes;
+        b->download_jobs();
+        float kms = 0;
+        CK(cudaEventElapsedTime(&kms, b->k0, b->k1));
+        kernel_ms += kms;
+        std::vector<int32_t> parked;
+        for (int32_t s : pending)
+          if (b->jobs[size_t(s)].status == ST_ARENA_FULL) parked.push_back(s);
+        if (parked.empty()) break;
+        if (slots == 1) throw AlignError{POA_ERR_ALLOC, "a read set needs more DP arena than the memory budget"};
+        for (int32_t s : parked) b->jobs[size_t(s)].status = ST_OK;
+        b->upload_jobs();
+        pending = parked;
+        slots = std::max<int64_t>(1, slots / 8);
+      }
+    } else {
+      // plain form: every read is its own launch, one warp, whole pool as arena
+      const int64_t slot_bytes = b->arena_pool / 256 * 256;
+      slots_first = 1;
+      CK(cudaEventRecord(b->k0, ctx->stream));
+      for (int64_t s = 0; s < b->n_sets; ++s) {
+        const int64_t k = b->set_off[s + 1] - b->set_off[s];
+        for (int64_t r = 0; r < k; ++r) {
+          CK(launch_extend_step(b->d_jobs + s, b->P, b->arenas, slot_bytes, int(r), ctx->stream));
+          ++launches;
+        }
+      }
+      CK(cudaEventRecord(b->k1, ctx->stream));
+      CK(cudaEventSynchronize(b->k1));
+      float kms = 0;
+      CK(cudaEventElapsedTime(&kms, b->k0, b->k1));
+      kernel_ms += kms;
+      passes = 1;
+    }
+    CK(cudaEventRecord(b->e1, ctx->stream));
+    CK(cudaEventSynchronize(b->e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+    b->download_jobs();
+    b->ran = true;
+    if (stats) {
+      uint64_t cells = 0, reads = 0, dpb = 0;
+      for (auto &J : b->jobs) {
+        cells += J.cells;
+        dpb += J.dp_bytes;
+        reads += uint64_t(J.next_read);
+      }
+      stats->cells = cells;
+      stats->dp_bytes = dpb;
+      stats->kernel_ms = kernel_ms;
+      stats->reads = reads;
+      stats->device_ms = ms;
+      stats->launches = launches;
+      stats->relaunches = passes - 1;
+      stats->slots = slots_first;
+    }
+  });
+}
+
+int poa_batch_status(poa_ctx *ctx, poa_batch *b, int64_t set, char **message) {
+  *message = nullptr;
+  int rc = POA_OK;
+  int api_rc = api(ctx, [&] {
+    if (set < 0 || set >= b->n_sets) throw AlignError{POA_ERR_INVALID, "set index out of range"};
+    const Job &J = b->jobs[size_t(set)];
+    if (J.status != ST_OK) {
+      rc = status_code(J.status);
+      *message = dup_string(status_message(J.status, J.err_i, J.err_j));
+    }
+  });
+  return api_rc != POA_OK ? api_rc : rc;
+}
+
+int poa_batch_output(poa_ctx *ctx, poa_batch *b, int64_t set, int32_t result, const char *const *names,
+                     const char *const *comments, char **out, int64_t *out_len) {
+  *out = nullptr;
+  *out_len = 0;
+  return api(ctx, [&] {
+    if (set < 0 || set >= b->n_sets) throw AlignError{POA_ERR_INVALID, "set index out of range"};
+    const Job &J = b->jobs[size_t(set)];
+    if (J.status != ST_OK) throw AlignError{status_code(J.status), status_message(J.status, J.err_i, J.err_j)};
+    auto gs = b->graphs({int32_t(set)});
+    const int64_t k = b->set_off[set + 1] - b->set_off[set];
+    auto nm = name_list(k, names, "read");
+    std::vector<std::string> cm(static_cast<size_t>(k));
+    for (int64_t i = 0; i < k && comments; ++i) cm[size_t(i)] = comments[i];
+    std::string s, err;
+    if (result == 0) {
+      std::vector<uint8_t> sq;
+      std::vector<int64_t> ids, cv;
+      gs[0].consensus(b->hp, sq, ids, cv);
+      s = ">consensus sequence\n" + std::string(sq.begin(), sq.end()) + "\n";
+    } else if (result == 1) {
+      if (!gs[0].msa(b->hp, nm, cm, s, err)) throw AlignError{POA_ERR_ALIGN, err};
+    } else if (result == 2) {
+      if (!gs[0].gfa(b->hp, nm, s, err)) throw AlignError{POA_ERR_ALIGN, err};
+    } else {
+      throw AlignError{POA_ERR_INVALID, "result format and verbosity must be 0..2"};
+    }
+    *out = dup_string(s);
+    *out_len = int64_t(s.size());
+  });
+}
+
+int poa_batch_output_all(poa_ctx *ctx, poa_batch *b, int32_t result, char **out, int64_t *out_len) {
+  *out = nullptr;
+  *out_len = 0;
+  return api(ctx, [&] {
+    if (result != 0 && result != 2) throw AlignError{POA_ERR_INVALID, "batch output supports results 0 and 2"};
+    std::vector<int32_t> ids(static_cast<size_t>(b->n_sets));
+    std::iota(ids.begin(), ids.end(), 0);
+    auto gs = b->graphs(ids);
+    std::vector<std::string> parts(ids.size());
+    const int nt = std::max(1, std::min<int>(int(std::thread::hardware_concurrency()), 32));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+      pool.emplace_back([&, t] {
+        for (size_t s = size_t(t); s < ids.size(); s += size_t(nt)) {
+          const Job &J = b->jobs[s];
+          if (J.status != ST_OK) {
+            parts[s] = "!error " + status_message(J.status, J.err_i, J.err_j) + "\n";
+            continue;
+          }
+          if (result == 0) {
+            std::vector<uint8_t> sq;
+            std::vector<int64_t> idv, cv;
+            gs[s].consensus(b->hp, sq, idv, cv);
+            parts[s] = ">consensus sequence\n" + std::string(sq.begin(), sq.end()) + "\n";
+          } else {
+            const int64_t k = b->set_off[s + 1] - b->set_off[s];
+            auto nm = name_list(k, nullptr, "read");
+            std::string err;
+            if (!gs[s].gfa(b->hp, nm, parts[s], err)) parts[s] = "!error " + err + "\n";
+          }
+        }
+      });
+    for (auto &th : pool) th.join();
+    size_t total = 0;
+    for (auto &p : parts) total += p.size();
+    std::string all;
+    all.reserve(total);
+    for (auto &p : parts) all += p;
+    *out = dup_string(all);
+    *out_len = int64_t(all.size());
+  });
+}
+
+int poa_batch_graph(poa_ctx *ctx, poa_batch *b, int64_t set, poa_graph **out) {
+  *out = nullptr;
+  return api(ctx, [&] {
+    if (set < 0 || set >= b->n_sets) throw AlignError{POA_ERR_INVALID, "set index out of range"};
+    b->download_jobs();
+    const Job &src = b->jobs[size_t(set)];
+    Caps c = b->caps[size_t(set)];
+    std::unique_ptr<poa_graph> g(new_graph(ctx, b->hp, c));
+    auto olda = arrays(src, c);
+    auto newa = arrays(g->h, g->caps);
+    for (size_t k = 0; k < olda.size(); ++k)
+      CK(cudaMemcpyAsync(newa[k].first, olda[k].first, olda[k].second, cudaMemcpyDeviceToDevice, ctx->stream));
+    Job nj = g->h;
+    nj.n_nodes = src.n_nodes;
+    nj.n_chunks = src.n_chunks;
+    nj.n_edges = src.n_edges;
+    nj.n_paths = src.n_paths;
+    nj.path_used = src.path_used;
+    nj.n_rank = src.n_rank;
+    nj.status = ST_OK;
+    nj.cells = src.cells;
+    g->h = nj;
+    g->upload();
+    g->sync();
+    *out = g.release();
+  });
+}
+
+int poa_batch_transfer_bytes(poa_ctx *ctx, poa_batch *b, uint64_t *h2d, uint64_t *d2h) {
+  return api(ctx, [&] {
+    *h2d = b->h2d_bytes;
+    *d2h = b->d2h_bytes;
+  });
+}
+
+void poa_batch_free(poa_batch *batch) { delete batch; }
+
+}  // extern "C"

@@ -1,0 +1,30 @@
+// Internal interface between the host runtime and the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "poa_device.cuh"
+
+namespace poa {
+
+// Launchers (poa_kernels.cu). All are asynchronous on `stream`.
+cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *queue, const DevParams &P,
+                         char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream);
+cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,
+                               cudaStream_t stream);
+cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *reads,
+                                const int64_t *read_off, const int32_t *read_len, int r0, int r1,
+                                cudaStream_t stream);
+cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q, int qlen,
+                         int mode, int beg_id, int end_id, int adaptive, uint64_t band_b, int retry, int4 *out,
+                         int32_t *out_n, cudaStream_t stream);
+cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, const int4 *items, int n,
+                            cudaStream_t stream);
+cudaError_t launch_add_node(Job *job_dev, int sigma, int base, cudaStream_t stream);
+cudaError_t launch_add_edge(Job *job_dev, int from, int to, cudaStream_t stream);
+cudaError_t launch_toposort(Job *job_dev, char *arena, int64_t bytes, cudaStream_t stream);
+cudaError_t launch_reset(Job *jobs_dev, int n_jobs, int sigma, int unknown, cudaStream_t stream);
+int kernel_launches_per_batch();
+
+}  // namespace poa

@@ -1,0 +1,204 @@
+// Kernels of the B200 POA library: the persistent batched read-loop kernel,
+// the plain one-read-per-launch kernel, and the single-graph operations behind
+// the reference-shaped C ABI. One warp per job; blocks of WARPS_PER_BLOCK
+// independent warps.
+#include "poa_internal.h"
+
+namespace poa {
+
+constexpr int WARPS_PER_BLOCK = 4;
+
+// Persistent batched kernel: each warp takes jobs from a size-ordered queue
+// (largest first) and runs their remaining reads. A job that outgrows the
+// warp's DP arena parks at its current read (graph untouched) for a later
+// pass with larger arenas.
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
+    k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *queue, DevParams P, char *arenas,
+            int64_t slot_bytes) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  char *arena = arenas + warp * slot_bytes;
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(queue, 1);
+    q = __shfl_sync(FULL, q, 0);
+    if (q >= n_jobs) break;
+    Job *J = jobs + order[q];
+    const int n_reads = J->n_reads;
+    for (int r = J->next_read; r < n_reads; ++r) {
+      const int32_t st = extend_one(J, P, arena, slot_bytes, J->reads + J->read_off[r], J->read_len[r], r);
+      if (st != ST_OK) {
+        if (lane == 0) J->status = st;
+        break;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Plain form: one launch aligns one read of one job.
+__global__ void k_extend_step(Job *J, DevParams P, char *arena, int64_t bytes, int r) {
+  if (J->status != ST_OK || J->next_read != r) return;
+  const int32_t st = extend_one(J, P, arena, bytes, J->reads + J->read_off[r], J->read_len[r], r);
+  if (st != ST_OK && (threadIdx.x & 31) == 0) J->status = st;
+}
+
+// extend_graph over reads r0..r1-1 held in a caller buffer.
+__global__ void k_extend_range(Job *J, DevParams P, char *arena, int64_t bytes, const uint8_t *reads,
+                               const int64_t *read_off, const int32_t *read_len, int r0, int r1) {
+  for (int r = r0; r < r1; ++r) {
+    const int32_t st = extend_one(J, P, arena, bytes, reads + read_off[r], read_len[r], r);
+    if (st != ST_OK) {
+      if ((threadIdx.x & 31) == 0) J->status = st;
+      return;
+    }
+  }
+}
+
+// align::align (mode 0) or align::poa / poa_inner (mode 1) without modifying
+// the graph; the path is copied to `out`.
+__global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const uint8_t *q, int qlen, int mode,
+                        int beg_id, int end_id, int adaptive, uint64_t band_b, int retry, int4 *out,
+                        int32_t *out_n) {
+  const int lane = threadIdx.x & 31;
+  Scratch s;
+  int n_items = 0;
+  Work cells{};
+  int32_t st;
+  if (mode == 0) {
+    st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells);
+  } else if (retry) {
+    st = poa_retry(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, s, &n_items, &cells);
+  } else {
+    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, P.f, s, &n_items, &cells);
+  }
+  if (st == ST_OK)
+    for (int k = lane; k < n_items; k += 32) out[k] = s.items[k];
+  if (lane == 0) {
+    J->status = st;
+    *out_n = st == ST_OK ? n_items : 0;
+    if (st == ST_OK) {
+      J->cells += cells.cells;
+      J->dp_bytes += cells.dp_bytes;
+    }
+  }
+}
+
+__global__ void k_add_path(Job *J, DevParams P, int seq_id, const int4 *items, int n) {
+  if (threadIdx.x == 0) J->status = add_path(J, P, seq_id, items, n);
+}
+
+__global__ void k_add_node(Job *J, int sigma, int base) {
+  if (threadIdx.x == 0) {
+    if (J->n_nodes + 1 > J->node_cap) {
+      J->status = ST_GRAPH_FULL;
+      return;
+    }
+    J->err_i = add_node(J, sigma, base);
+    J->status = ST_OK;
+  }
+}
+
+__global__ void k_add_edge(Job *J, int from, int to) {
+  if (threadIdx.x == 0) {
+    if (J->n_chunks + 2 > J->chunk_cap) {
+      J->status = ST_GRAPH_FULL;
+      return;
+    }
+    add_edge(J, from, to);
+    J->status = ST_OK;
+  }
+}
+
+__global__ void k_toposort(Job *J, char *arena, int64_t bytes) {
+  if (threadIdx.x == 0) {
+    if (int64_t(J->n_nodes) * 8 > bytes) {
+      J->status = ST_ARENA_FULL;
+      return;
+    }
+    int32_t *deg = reinterpret_cast<int32_t *>(arena);
+    J->status = toposort(J, deg, deg + J->n_nodes);
+  }
+}
+
+// Graph::new (graph.rs:30-40) for every job: source and sink, no edges, no
+// rank, no paths; the read loop restarts at read 0.
+__global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_jobs) return;
+  Job *J = jobs + j;
+  J->n_nodes = 0;
+  J->n_chunks = 0;
+  J->n_edges = 0;
+  J->n_paths = 0;
+  J->path_used = 0;
+  J->n_rank = 0;
+  J->path_off[0] = 0;
+  add_node(J, sigma, unknown);
+  add_node(J, sigma, unknown);
+  J->next_read = 0;
+  J->status = ST_OK;
+  J->err_i = J->err_j = 0;
+  J->n_items = 0;
+  J->cells = 0;
+  J->dp_bytes = 0;
+}
+
+cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *queue, const DevParams &P,
+                         char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
+  const int blocks = (slots + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+  k_batch<<<blocks, WARPS_PER_BLOCK * 32, 0, stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, queue, P, arenas,
+                                                         slot_bytes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,
+                               cudaStream_t stream) {
+  k_extend_step<<<1, 32, 0, stream>>>(job_dev, P, arena, bytes, read);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *reads,
+                                const int64_t *read_off, const int32_t *read_len, int r0, int r1,
+                                cudaStream_t stream) {
+  k_extend_range<<<1, 32, 0, stream>>>(job_dev, P, arena, bytes, reads, read_off, read_len, r0, r1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q, int qlen,
+                         int mode, int beg_id, int end_id, int adaptive, uint64_t band_b, int retry, int4 *out,
+                         int32_t *out_n, cudaStream_t stream) {
+  k_align<<<1, 32, 0, stream>>>(job_dev, P, arena, bytes, q, qlen, mode, beg_id, end_id, adaptive, band_b, retry,
+                                 out, out_n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, const int4 *items, int n,
+                            cudaStream_t stream) {
+  k_add_path<<<1, 32, 0, stream>>>(job_dev, P, seq_id, items, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_node(Job *job_dev, int sigma, int base, cudaStream_t stream) {
+  k_add_node<<<1, 32, 0, stream>>>(job_dev, sigma, base);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_edge(Job *job_dev, int from, int to, cudaStream_t stream) {
+  k_add_edge<<<1, 32, 0, stream>>>(job_dev, from, to);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_toposort(Job *job_dev, char *arena, int64_t bytes, cudaStream_t stream) {
+  k_toposort<<<1, 32, 0, stream>>>(job_dev, arena, bytes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reset(Job *jobs_dev, int n_jobs, int sigma, int unknown, cudaStream_t stream) {
+  k_reset<<<(n_jobs + 127) / 128, 128, 0, stream>>>(jobs_dev, n_jobs, sigma, unknown);
+  return cudaGetLastError();
+}
+
+int kernel_launches_per_batch() { return 1; }
+
+}  // namespace poa

@@ -1,0 +1,358 @@
+"""Host API mirroring the minipoa-rs library (src/lib.rs, src/align.rs,
+src/graph.rs) on top of the C ABI. The DP, traceback, fusion and toposort run
+on the B200; this module only marshals arguments and results.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import List, Optional, Sequence as Seq, Tuple
+
+from . import _lib
+from .params import AlignedBase, Params, Sequence
+
+
+class PoaError(RuntimeError):
+    """A failed call; `code` is the POA_ERR_* status, str() the message."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def dp_backend() -> str:
+    """lib.rs:15"""
+    return _lib.load().poa_dp_backend().decode()
+
+
+def _bytes(x) -> bytes:
+    return x.encode() if isinstance(x, str) else bytes(x)
+
+
+def _seq_arrays(seqs: Seq[bytes]):
+    seqs = [_bytes(s) for s in seqs]
+    bufs = [(ctypes.c_uint8 * max(1, len(s))).from_buffer_copy(s if s else b"\0") for s in seqs]
+    arr = (ctypes.POINTER(ctypes.c_uint8) * max(1, len(seqs)))(
+        *[ctypes.cast(b, ctypes.POINTER(ctypes.c_uint8)) for b in bufs])
+    lens = (ctypes.c_int64 * max(1, len(seqs)))(*[len(s) for s in seqs])
+    return arr, lens, bufs
+
+
+class Context:
+    """One CUDA device with a stream, a DP arena and a memory budget."""
+
+    def __init__(self, device: int = 0, mem_budget: int = 0):
+        self.L = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.L.poa_ctx_create(device, mem_budget, ctypes.byref(h))
+        if rc != 0:
+            raise PoaError(rc, self.L.poa_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.poa_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int):
+        if rc != 0:
+            raise PoaError(rc, self.L.poa_last_error(self.h).decode())
+
+    def validate(self, params: Params) -> Optional[str]:
+        c, keep = params.to_c()
+        rc = self.L.poa_params_validate(self.h, ctypes.byref(c))
+        return None if rc == 0 else self.L.poa_last_error(self.h).decode()
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context()
+    return _default_ctx
+
+
+def _items_to_list(ptr, n) -> List[AlignedBase]:
+    out = []
+    for k in range(n):
+        it = ptr[k]
+        out.append(AlignedBase(None if it.node < 0 else it.node, it.base, None if it.aligned < 0 else it.aligned))
+    return out
+
+
+class Graph:
+    """graph.rs Graph, resident in device memory."""
+
+    def __init__(self, params: Optional[Params] = None, ctx: Optional[Context] = None, handle=None):
+        self.ctx = ctx or default_context()
+        self.L = self.ctx.L
+        if handle is None:
+            c, keep = (params or Params()).to_c()
+            h = ctypes.c_void_p()
+            self.ctx.check(self.L.poa_graph_new(self.ctx.h, ctypes.byref(c), ctypes.byref(h)))
+            handle = h
+        self.h = handle
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.L.poa_graph_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    # graph.rs:82
+    def add_path(self, seq_id: int, path: Seq) -> None:
+        arr = (_lib.AlignedBaseC * max(1, len(path)))()
+        for k, it in enumerate(path):
+            node, base, aligned = (it.node, it.base, it.aligned) if isinstance(it, AlignedBase) else it
+            arr[k].node = -1 if node is None else node
+            arr[k].base = base
+            arr[k].aligned = -1 if aligned is None else aligned
+        self.ctx.check(self.L.poa_graph_add_path(self.ctx.h, self.h, seq_id, arr, len(path)))
+
+    # graph.rs:42
+    def add_node(self, base: int) -> int:
+        out = ctypes.c_int64()
+        self.ctx.check(self.L.poa_graph_add_node(self.ctx.h, self.h, base, ctypes.byref(out)))
+        return out.value
+
+    # graph.rs:62
+    def add_edge(self, a: int, b: int) -> None:
+        self.ctx.check(self.L.poa_graph_add_edge(self.ctx.h, self.h, a, b))
+
+    # graph.rs:125
+    def toposort(self, grouped: bool = False) -> None:
+        self.ctx.check(self.L.poa_graph_toposort(self.ctx.h, self.h, int(grouped)))
+
+    # graph.rs:181
+    def consensus(self, params: Params) -> Tuple[bytes, List[int], List[int]]:
+        c, keep = params.to_c()
+        s = ctypes.POINTER(ctypes.c_uint8)()
+        ids = ctypes.POINTER(ctypes.c_int64)()
+        cov = ctypes.POINTER(ctypes.c_int64)()
+        n = ctypes.c_int64()
+        self.ctx.check(self.L.poa_graph_consensus(self.ctx.h, ctypes.byref(c), self.h, ctypes.byref(s),
+                                                  ctypes.byref(ids), ctypes.byref(cov), ctypes.byref(n)))
+        try:
+            return bytes(s[: n.value]), [ids[i] for i in range(n.value)], [cov[i] for i in range(n.value)]
+        finally:
+            for p in (s, ids, cov):
+                self.L.poa_free(ctypes.cast(p, ctypes.c_void_p))
+
+    def _text(self, fn, *args) -> str:
+        out = ctypes.c_char_p()
+        n = ctypes.c_int64()
+        self.ctx.check(fn(*args, ctypes.byref(out), ctypes.byref(n)))
+        try:
+            return ctypes.string_at(out, n.value).decode()
+        finally:
+            self.L.poa_free(ctypes.cast(out, ctypes.c_void_p))
+
+    # graph.rs:239
+    def msa(self, params: Params, sequences: Seq[Sequence]) -> str:
+        c, keep = params.to_c()
+        names = (ctypes.c_char_p * max(1, len(sequences)))(*[s.name.encode() for s in sequences])
+        comments = (ctypes.c_char_p * max(1, len(sequences)))(*[s.comment.encode() for s in sequences])
+        return self._text(self.L.poa_graph_msa, self.ctx.h, ctypes.byref(c), self.h, len(sequences), names,
+                          comments)
+
+    # graph.rs:281
+    def gfa(self, params: Params, sequences: Seq[Sequence]) -> str:
+        c, keep = params.to_c()
+        names = (ctypes.c_char_p * max(1, len(sequences)))(*[s.name.encode() for s in sequences])
+        return self._text(self.L.poa_graph_gfa, self.ctx.h, ctypes.byref(c), self.h, len(sequences), names)
+
+    def sizes(self) -> _lib.GraphSizes:
+        s = _lib.GraphSizes()
+        self.ctx.check(self.L.poa_graph_sizes_get(self.ctx.h, self.h, ctypes.byref(s)))
+        return s
+
+    def n_nodes(self) -> int:
+        return self.sizes().n_nodes
+
+    def dump(self) -> dict:
+        """Every public graph field (graph.rs:6-27) as plain lists, in the
+        same shape as the oracle's dump."""
+        s = self.sizes()
+        n, e, npth, pit, sig = s.n_nodes, s.n_edges, s.n_paths, s.path_items, s.alphabet
+        A = lambda k: (ctypes.c_int64 * max(1, k))()  # noqa: E731
+        fields, rank, aligned = A(4 * n), A(n), A(n * sig)
+        icnt, ocnt, ipairs, opairs = A(n), A(n), A(2 * e), A(2 * e)
+        pseq, plen, pids = A(npth), A(npth), A(pit)
+        self.ctx.check(self.L.poa_graph_export(self.ctx.h, self.h, fields, rank, aligned, icnt, ocnt, ipairs,
+                                               opairs, pseq, plen, pids))
+        incoming, outgoing = [], []
+        a = b = 0
+        for i in range(n):
+            incoming.append([(ipairs[a + 2 * k], ipairs[a + 2 * k + 1]) for k in range(icnt[i])])
+            a += 2 * icnt[i]
+            outgoing.append([(opairs[b + 2 * k], opairs[b + 2 * k + 1]) for k in range(ocnt[i])])
+            b += 2 * ocnt[i]
+        paths, c = [], 0
+        for i in range(npth):
+            paths.append((pseq[i], list(pids[c:c + plen[i]])))
+            c += plen[i]
+        return {
+            "base": [fields[4 * i] for i in range(n)],
+            "parent": [fields[4 * i + 1] for i in range(n)],
+            "rank_of": [fields[4 * i + 2] for i in range(n)],
+            "coverage": [fields[4 * i + 3] for i in range(n)],
+            "incoming": incoming,
+            "outgoing": outgoing,
+            "rank": list(rank[:s.n_rank]),
+            "aligned": [list(aligned[i * sig:(i + 1) * sig]) for i in range(n)],
+            "paths": paths,
+        }
+
+
+def _call_path(ctx, fn, *args) -> List[AlignedBase]:
+    out = ctypes.POINTER(_lib.AlignedBaseC)()
+    n = ctypes.c_int64()
+    ctx.check(fn(*args, ctypes.byref(out), ctypes.byref(n)))
+    try:
+        return _items_to_list(out, n.value)
+    finally:
+        ctx.L.poa_free(ctypes.cast(out, ctypes.c_void_p))
+
+
+def align(params: Params, graph: Graph, query: bytes) -> List[AlignedBase]:
+    """align.rs:81"""
+    c, keep = params.to_c()
+    q = _bytes(query)
+    qb = (ctypes.c_uint8 * max(1, len(q))).from_buffer_copy(q if q else b"\0")
+    return _call_path(graph.ctx, graph.L.poa_align, graph.ctx.h, ctypes.byref(c), graph.h, qb, len(q))
+
+
+def poa(params: Params, graph: Graph, beg_id: int, end_id: int, query: bytes, adaptive: bool, band_b: int,
+        kernel: int = 0, retry: bool = True) -> List[AlignedBase]:
+    """align.rs:192 (retry=True) / poa_inner and a forced kernel (retry=False,
+    kernel 1 = i32, 2 = i64)."""
+    c, keep = params.to_c()
+    q = _bytes(query)
+    qb = (ctypes.c_uint8 * max(1, len(q))).from_buffer_copy(q if q else b"\0")
+    return _call_path(graph.ctx, graph.L.poa_poa, graph.ctx.h, ctypes.byref(c), graph.h, beg_id, end_id, qb,
+                      len(q), int(adaptive), band_b, kernel, int(retry))
+
+
+def align_sequences(params: Params, sequences: Seq, ctx: Optional[Context] = None) -> Graph:
+    """lib.rs:177. `sequences` are Sequence records or raw bytes."""
+    ctx = ctx or default_context()
+    raw = [s.seq if isinstance(s, Sequence) else _bytes(s) for s in sequences]
+    c, keep = params.to_c()
+    arr, lens, bufs = _seq_arrays(raw)
+    h = ctypes.c_void_p()
+    ctx.check(ctx.L.poa_align_sequences(ctx.h, ctypes.byref(c), len(raw), arr, lens, ctypes.byref(h)))
+    return Graph(ctx=ctx, handle=h)
+
+
+def extend_graph(params: Params, graph: Graph, sequences: Seq, existing: int) -> None:
+    """lib.rs:184"""
+    raw = [s.seq if isinstance(s, Sequence) else _bytes(s) for s in sequences]
+    c, keep = params.to_c()
+    arr, lens, bufs = _seq_arrays(raw)
+    graph.ctx.check(graph.L.poa_extend_graph(graph.ctx.h, ctypes.byref(c), graph.h, len(raw), arr, lens, existing))
+
+
+def run(params: Params, sequences: Seq[Sequence], ctx: Optional[Context] = None) -> str:
+    """lib.rs:207-242 after input parsing: RNA detection, the read loop and
+    the selected output (params.result: 0 consensus, 1 MSA, 2 GFA)."""
+    if not sequences:
+        raise PoaError(_lib.POA_ERR_INVALID, "input contains no sequences")
+    params = params.copy()
+    params.is_rna = len(params.alphabet) <= 5 and any(b"U" in s.seq.upper() for s in sequences)
+    g = align_sequences(params, sequences, ctx)
+    if params.result == 0:
+        return ">consensus sequence\n" + g.consensus(params)[0].decode() + "\n"
+    if params.result == 1:
+        return g.msa(params, sequences)
+    return g.gfa(params, sequences)
+
+
+class Batch:
+    """Independent read sets resident on the device; one run aligns them all
+    (mode 0: persistent batched kernel, mode 1: one launch per read)."""
+
+    def __init__(self, params: Params, sets: List[List[bytes]], ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.L = self.ctx.L
+        self.params = params
+        flat = [_bytes(s) for st in sets for s in st]
+        off = [0]
+        for st in sets:
+            off.append(off[-1] + len(st))
+        self.n_sets = len(sets)
+        self.set_sizes = [len(st) for st in sets]
+        c, keep = params.to_c()
+        arr, lens, bufs = _seq_arrays(flat)
+        offs = (ctypes.c_int64 * len(off))(*off)
+        h = ctypes.c_void_p()
+        self.ctx.check(self.L.poa_batch_create(self.ctx.h, ctypes.byref(c), len(sets), offs, arr, lens,
+                                               ctypes.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.L.poa_batch_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def tune(self, warps_per_sm: int = 0, arena_bytes_per_slot: int = 0):
+        self.ctx.check(self.L.poa_batch_tune(self.ctx.h, self.h, warps_per_sm, arena_bytes_per_slot))
+
+    def run(self, mode: int = 0) -> _lib.BatchStats:
+        st = _lib.BatchStats()
+        self.ctx.check(self.L.poa_batch_run(self.ctx.h, self.h, mode, ctypes.byref(st)))
+        return st
+
+    def status(self, s: int) -> Optional[str]:
+        msg = ctypes.c_char_p()
+        rc = self.L.poa_batch_status(self.ctx.h, self.h, s, ctypes.byref(msg))
+        if rc == 0:
+            return None
+        text = msg.value.decode() if msg.value else self.L.poa_last_error(self.ctx.h).decode()
+        if msg:
+            self.L.poa_free(ctypes.cast(msg, ctypes.c_void_p))
+        return text
+
+    def output(self, s: int, result: int, sequences: Optional[Seq[Sequence]] = None) -> str:
+        out = ctypes.c_char_p()
+        n = ctypes.c_int64()
+        names = comments = None
+        if sequences is not None:
+            names = (ctypes.c_char_p * max(1, len(sequences)))(*[x.name.encode() for x in sequences])
+            comments = (ctypes.c_char_p * max(1, len(sequences)))(*[x.comment.encode() for x in sequences])
+        self.ctx.check(self.L.poa_batch_output(self.ctx.h, self.h, s, result, names, comments, ctypes.byref(out),
+                                               ctypes.byref(n)))
+        try:
+            return ctypes.string_at(out, n.value).decode()
+        finally:
+            self.L.poa_free(ctypes.cast(out, ctypes.c_void_p))
+
+    def output_all(self, result: int) -> bytes:
+        out = ctypes.c_char_p()
+        n = ctypes.c_int64()
+        self.ctx.check(self.L.poa_batch_output_all(self.ctx.h, self.h, result, ctypes.byref(out), ctypes.byref(n)))
+        try:
+            return ctypes.string_at(out, n.value)
+        finally:
+            self.L.poa_free(ctypes.cast(out, ctypes.c_void_p))
+
+    def transfer_bytes(self):
+        h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(self.L.poa_batch_transfer_bytes(self.ctx.h, self.h, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return h2d.value, d2h.value
+
+    def graph(self, s: int) -> Graph:
+        h = ctypes.c_void_p()
+        self.ctx.check(self.L.poa_batch_graph(self.ctx.h, self.h, s, ctypes.byref(h)))
+        return Graph(ctx=self.ctx, handle=h)

@@ -105,6 +105,7 @@ void orc_graph_node_fields(const void *g, int64_t *out);
 int64_t orc_graph_edge_total(const void *g);
 void orc_graph_edges(const void *g, int64_t *in_cnt, int64_t *out_cnt, int64_t *in_pairs, int64_t *out_pairs);
 void orc_graph_rank(const void *g, int64_t *out);
+int64_t orc_graph_rank_len(const void *g);
 /* aligned[] groups: n * alphabet entries, -1 = None */
 void orc_graph_aligned(const void *g, int64_t *out);
 /* paths: seq ids (n_paths), lengths (n_paths), then concatenated ids */

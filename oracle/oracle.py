@@ -89,6 +89,8 @@ def lib():
         L.orc_graph_edge_total.restype = i64
         L.orc_graph_edges.argtypes = [vp, P(i64), P(i64), P(i64), P(i64)]
         L.orc_graph_rank.argtypes = [vp, P(i64)]
+        L.orc_graph_rank_len.argtypes = [vp]
+        L.orc_graph_rank_len.restype = i64
         L.orc_graph_aligned.argtypes = [vp, P(i64)]
         L.orc_graph_path_total.argtypes = [vp]
         L.orc_graph_path_total.restype = i64
@@ -258,7 +260,8 @@ class OracleGraph:
         ip = (ctypes.c_int64 * max(1, 2 * e))()
         op = (ctypes.c_int64 * max(1, 2 * e))()
         L.orc_graph_edges(self.h, ic, oc, ip, op)
-        rk = (ctypes.c_int64 * n)()
+        nr = L.orc_graph_rank_len(self.h)
+        rk = (ctypes.c_int64 * max(1, nr))()
         L.orc_graph_rank(self.h, rk)
         al = (ctypes.c_int64 * (n * alphabet_size))()
         L.orc_graph_aligned(self.h, al)
@@ -287,7 +290,7 @@ class OracleGraph:
             "coverage": [f[4 * i + 3] for i in range(n)],
             "incoming": incoming,
             "outgoing": outgoing,
-            "rank": list(rk[:n]),
+            "rank": list(rk[:nr]),
             "aligned": [list(al[i * alphabet_size:(i + 1) * alphabet_size]) for i in range(n)],
             "paths": paths,
         }

@@ -244,14 +244,17 @@ struct Graph {
       stack.pop_back();
       usize r = rank.size();
       rank.push_back(id);
+      usize single = id;
+      const usize *mem_begin = &single, *mem_end = &single + 1;
       std::vector<usize> members;
       if (grouped) {
         for (i64 a : nodes[id].aligned)
           if (a != NONE) members.push_back(usize(a));
-      } else {
-        members.push_back(id);
+        mem_begin = members.data();
+        mem_end = members.data() + members.size();
       }
-      for (usize member : members) {
+      for (const usize *mp = mem_begin; mp != mem_end; ++mp) {
+        usize member = *mp;
         nodes[member].rank = r;
         visited += 1;
         for (usize next : nodes[member].outgoing) {
@@ -903,25 +906,32 @@ static std::vector<AlignedBase> poa_i64(const Params &params, const Graph &graph
 // AVX2 8-lane i32 kernel pieces (the timed CPU baseline). They mirror the
 // reference's wide::i32x8 organisation (align.rs:459-491, 755-845).
 
-__attribute__((target("avx2"))) static inline __m256i shift_lanes(__m256i v, int k) {
-  // lanes shifted up by k, low k lanes filled with SHIFT_FILL
-  alignas(32) static const int32_t idx[4][8] = {
-      {0, 0, 1, 2, 3, 4, 5, 6}, {0, 0, 0, 1, 2, 3, 4, 5}, {0, 0, 0, 0, 0, 1, 2, 3}, {0, 0, 0, 0, 0, 0, 0, 0}};
-  int sel = k == 1 ? 0 : (k == 2 ? 1 : 2);
-  __m256i perm = _mm256_permutevar8x32_epi32(v, _mm256_load_si256((const __m256i *)idx[sel]));
-  __m256i lane = _mm256_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7);
-  __m256i mask = _mm256_cmpgt_epi32(_mm256_set1_epi32(k), lane);
-  return _mm256_blendv_epi8(perm, _mm256_set1_epi32(SHIFT_FILL), mask);
+// Lanes shifted up by 1, 2 or 4 with SHIFT_FILL in the vacated low lanes.
+__attribute__((target("avx2"))) static inline __m256i shift1(__m256i v, __m256i fill) {
+  return _mm256_blend_epi32(_mm256_permutevar8x32_epi32(v, _mm256_setr_epi32(0, 0, 1, 2, 3, 4, 5, 6)), fill, 0x01);
+}
+__attribute__((target("avx2"))) static inline __m256i shift2(__m256i v, __m256i fill) {
+  return _mm256_blend_epi32(_mm256_permutevar8x32_epi32(v, _mm256_setr_epi32(0, 0, 0, 1, 2, 3, 4, 5)), fill, 0x03);
+}
+__attribute__((target("avx2"))) static inline __m256i shift4(__m256i v, __m256i fill) {
+  return _mm256_blend_epi32(_mm256_permutevar8x32_epi32(v, _mm256_setr_epi32(0, 0, 0, 0, 0, 1, 2, 3)), fill, 0x0F);
+}
+
+// Three shift stages give the within-block max-plus prefix; the carried-in
+// insertion state is added as a broadcast (align.rs:459-491).
+__attribute__((target("avx2"))) static inline __m256i insertion_prefix_v(__m256i md, __m256i carryv, i32 open,
+                                                                         i32 ext) {
+  const __m256i fill = _mm256_set1_epi32(SHIFT_FILL);
+  __m256i v = _mm256_add_epi32(md, _mm256_set1_epi32(open));
+  v = _mm256_max_epi32(v, _mm256_add_epi32(shift1(v, fill), _mm256_set1_epi32(ext)));
+  v = _mm256_max_epi32(v, _mm256_add_epi32(shift2(v, fill), _mm256_set1_epi32(ext * 2)));
+  v = _mm256_max_epi32(v, _mm256_add_epi32(shift4(v, fill), _mm256_set1_epi32(ext * 4)));
+  const __m256i ramp = _mm256_setr_epi32(ext, ext * 2, ext * 3, ext * 4, ext * 5, ext * 6, ext * 7, ext * 8);
+  return _mm256_max_epi32(v, _mm256_add_epi32(carryv, ramp));
 }
 
 __attribute__((target("avx2"))) static inline __m256i insertion_prefix(__m256i md, i32 carry, i32 open, i32 ext) {
-  __m256i v = _mm256_add_epi32(md, _mm256_set1_epi32(open));
-  v = _mm256_max_epi32(v, _mm256_add_epi32(shift_lanes(v, 1), _mm256_set1_epi32(ext)));
-  v = _mm256_max_epi32(v, _mm256_add_epi32(shift_lanes(v, 2), _mm256_set1_epi32(ext * 2)));
-  v = _mm256_max_epi32(v, _mm256_add_epi32(shift_lanes(v, 4), _mm256_set1_epi32(ext * 4)));
-  __m256i c = _mm256_add_epi32(_mm256_set1_epi32(carry), _mm256_setr_epi32(ext, ext * 2, ext * 3, ext * 4, ext * 5,
-                                                                             ext * 6, ext * 7, ext * 8));
-  return _mm256_max_epi32(v, c);
+  return insertion_prefix_v(md, _mm256_set1_epi32(carry), open, ext);
 }
 
 __attribute__((target("avx2"))) static void avx2_row_preds(std::vector<i32> &data, const FastRow &row,
@@ -948,18 +958,19 @@ __attribute__((target("avx2"))) static void avx2_row_preds(std::vector<i32> &dat
 __attribute__((target("avx2"))) static void avx2_row_scan(std::vector<i32> &data, const FastRow &row,
                                                           const i32 *profile, i32 open, i32 ext) {
   i32 *d = data.data();
-  i32 carry = NEG32;
+  __m256i carryv = _mm256_set1_epi32(NEG32);
+  const __m256i up1 = _mm256_setr_epi32(0, 0, 1, 2, 3, 4, 5, 6);
+  const __m256i last = _mm256_set1_epi32(7);
   for (usize local = 0; local < row.len; local += WIDTH) {
     __m256i diag = _mm256_add_epi32(_mm256_loadu_si256((const __m256i *)(d + row.m_offset + local)),
                                     _mm256_loadu_si256((const __m256i *)(profile + local)));
     __m256i md = _mm256_max_epi32(diag, _mm256_loadu_si256((const __m256i *)(d + row.d_offset + local)));
-    __m256i next = insertion_prefix(md, carry, open, ext);
-    alignas(32) i32 a[8];
-    _mm256_store_si256((__m256i *)a, next);
-    __m256i cur = _mm256_setr_epi32(carry, a[0], a[1], a[2], a[3], a[4], a[5], a[6]);
+    __m256i next = insertion_prefix_v(md, carryv, open, ext);
+    // current I = [carry, next[0..6]]; the next carry is next[7] broadcast
+    __m256i cur = _mm256_blend_epi32(_mm256_permutevar8x32_epi32(next, up1), carryv, 0x01);
     _mm256_storeu_si256((__m256i *)(d + row.i_offset + local), cur);
     _mm256_storeu_si256((__m256i *)(d + row.m_offset + local), _mm256_max_epi32(md, cur));
-    carry = a[7];
+    carryv = _mm256_permutevar8x32_epi32(next, last);
   }
 }
 
@@ -1248,6 +1259,7 @@ void orc_graph_rank(const void *g, int64_t *out) {
   const Graph &gr = *(const Graph *)g;
   for (size_t i = 0; i < gr.rank.size(); ++i) out[i] = int64_t(gr.rank[i]);
 }
+int64_t orc_graph_rank_len(const void *g) { return int64_t(((const Graph *)g)->rank.size()); }
 void orc_graph_aligned(const void *g, int64_t *out) {
   const Graph &gr = *(const Graph *)g;
   size_t a = 0;
