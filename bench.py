@@ -19,6 +19,7 @@ scaling, no collective on the data path); value = all ranks' cells / the
 slowest rank's time.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -230,6 +231,10 @@ def main():
     steps = []
     for _ in range(args.steps):
         steps.append(batch.run(0))
+        s = steps[-1]
+        print(f"[bench] rank {rank} step: {s.cells / 1e9:.2f} G cells, {s.device_ms:.1f} ms device, "
+              f"{s.kernel_ms:.1f} ms kernel, {s.cells / s.device_ms / 1e6:.1f} GCUPS, passes {1 + s.relaunches}, "
+              f"slots {s.slots}", file=sys.stderr, flush=True)
     clock_info = clocks.stop()
     barrier(pg)
     dev_ms = sum(s.device_ms for s in steps)
@@ -241,6 +246,9 @@ def main():
     all_cells = reduce_sum(pg, float(cells))
     value = all_cells / (max_ms / 1e3) / 1e9
     reads = sum(s.reads for s in steps)
+    first_slots, first_passes = steps[0].slots, steps[0].relaunches
+    del batch  # releases its DP arena pool before the end-to-end leg
+    gc.collect()
 
     # end to end through the C ABI from host buffers
     e2e_vals, h2d, d2h = [], 0, 0
@@ -293,8 +301,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "sets": args.sets, "seed": args.seed, "reads_per_step": reads // args.steps,
                        "cells_per_step": cells // args.steps, "l2": "inputs larger than L2 (no flush needed)",
-                       "parallelism": f"{world} independent GPU(s)", "slots": steps[0].slots,
-                       "relaunch_passes": steps[0].relaunches, "reads_per_s": reads / (dev_ms / 1e3)},
+                       "parallelism": f"{world} independent GPU(s)", "slots": first_slots,
+                       "relaunch_passes": first_passes, "reads_per_s": reads / (dev_ms / 1e3)},
             "roofline": roofline,
             "cpu_baseline": cb,
             "e2e": {"value": e2e_v, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -1,11 +1,14 @@
 // Device-side partial-order alignment for sm_100a.
 //
-// One warp owns one alignment job at a time. The DP row of a graph node is
-// computed by the warp across query columns (32-column chunks, one column per
-// lane); the query-direction affine gap is a warp-shuffle max-plus prefix
-// scan. The serial parts of the read loop (band-guide passes, traceback,
-// read-into-graph fusion, LIFO toposort) run on lane 0 against the job's
-// device-resident graph, so no graph crosses PCIe between reads.
+// One warp owns one alignment job at a time. A DP row (one graph node) is a
+// blocked register tile: each lane owns a run of consecutive query columns,
+// scans it serially, and one warp-shuffle max-plus scan over the lane
+// aggregates carries the query-direction affine gap across lanes.
+// Predecessor rows are read from a per-warp shared-memory ring of recent
+// rows. The band guides gather their lists warp-parallel; the serial parts
+// of the read loop (guide passes, traceback, read-into-graph fusion) run on
+// lane 0 against the job's device-resident graph, so no graph crosses PCIe
+// between reads.
 //
 // Semantics restated from minipoa-rs: src/align.rs (poa, poa_inner, both DP
 // kernels, traceback, push_diagonal), src/graph.rs (add_node, add_edge,
@@ -61,6 +64,7 @@ struct DevParams {
   int32_t adaptive;
   int32_t kernel;         // 0 = score-guard dispatch, 1 = i32 only, 2 = i64 only
   int32_t seeding;
+  int32_t relaxed_order;  // read loops may keep a spliced order between reads
   uint64_t b, f;
   uint64_t largest;       // max(|matrix|, |O|, |E|) of i32_scores_safe
 };
@@ -93,8 +97,9 @@ struct Job {
   int32_t n_reads, next_read;
   // outcome
   int32_t status, err_i, err_j, n_items;
-  uint64_t cells;     // DP cells of completed reads (retries included)
-  uint64_t dp_bytes;  // DP state bytes stored for those cells (M, D, I)
+  int32_t order_exact;  // 1 when rank is the reference's LIFO toposort order
+  uint64_t cells;       // DP cells of completed reads (retries included)
+  uint64_t dp_bytes;    // DP state bytes stored for those cells (M, D, I)
 };
 
 // Work counted by one alignment: 8-aligned band cells and the bytes of DP
@@ -108,11 +113,14 @@ struct Scratch {
   int64_t *head, *tail, *support, *row_off, *wsum;
   int64_t *peak, *streak, *peak_left, *peak_right, *offset_left, *offset_right, *extra;
   int32_t *row_start, *row_len, *pred_start, *pred_cnt, *succ_start, *succ_cnt;
-  int2 *pred;      // (row, weight) in incoming order, band-guide filtered
-  int32_t *succ;   // successor rows in outgoing order, range filtered
-  int32_t *seq;    // encoded, padded query
-  int4 *items;     // alignment result (node, base, aligned, -)
-  char *dp;        // DP matrix cells
+  int2 *pred;          // (row, weight) in incoming order; row = -1 once head is NEG
+  int2 *succ;          // (row, weight) in outgoing order, range filtered
+  int32_t *row_base;   // base code a row scores with (N for the last row)
+  int4 *pmeta;         // per pred entry: (row, band start, band length, -)
+  int64_t *pmeta_off;  // per pred entry: the predecessor row's arena offset
+  int32_t *seq;        // encoded, padded query
+  int4 *items;         // alignment result (node, base, aligned, resolved id)
+  char *dp;            // DP matrix cells
   int64_t dp_bytes;
 };
 
@@ -148,7 +156,10 @@ __device__ inline bool carve_scratch(char *arena, int64_t bytes, int n, int e, i
   s.succ_start = (int32_t *)take(N * 4);
   s.succ_cnt = (int32_t *)take(N * 4);
   s.pred = (int2 *)take(int64_t(e + 1) * 8);
-  s.succ = (int32_t *)take(int64_t(e + 1) * 4);
+  s.succ = (int2 *)take(int64_t(e + 1) * 8);
+  s.row_base = (int32_t *)take(N * 4);
+  s.pmeta = (int4 *)take(int64_t(e + 1) * 16);
+  s.pmeta_off = (int64_t *)take(int64_t(e + 1) * 8);
   s.seq = (int32_t *)take((padded + 32) * 4);
   s.items = (int4 *)take((n_items + 1) * 16);
   s.dp = arena + o;
@@ -230,8 +241,9 @@ __device__ inline void for_list(const Job *J, const int32_t *head, const int32_t
   }
 }
 
-// graph.rs:82-122 (lane 0). Capacity is checked before any change.
-__device__ inline int32_t add_path(Job *J, const DevParams &P, int seq_id, const int4 *items, int n) {
+// graph.rs:82-122 (lane 0). Capacity is checked before any change. The
+// resolved node id of each item is written to its .w field.
+__device__ inline int32_t add_path(Job *J, const DevParams &P, int seq_id, int4 *items, int n) {
   for (int t = 0; t < n; ++t) {
     const int4 it = items[t];
     if (it.y < 0 || it.y >= P.sigma) return ST_BASE_OUTSIDE;
@@ -261,6 +273,7 @@ __device__ inline int32_t add_path(Job *J, const DevParams &P, int seq_id, const
     }
     if (previous >= 0) add_edge(J, previous, id);
     previous = id;
+    items[t].w = id;
     if (id >= 2) J->path_items[J->path_used++] = id;
   }
   add_edge(J, previous >= 0 ? previous : 0, 1);
@@ -337,84 +350,147 @@ __device__ __forceinline__ T mins(T a, T b) {
   return a < b ? a : b;
 }
 
-// Band-guide passes of align.rs:623-680 (lane 0). Builds each row's filtered
-// predecessor list (incoming order, in-range, head != NEG), its total
-// incoming weight, and its range-filtered successor list.
-__device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int n) {
-  for (int i = 0; i < n; ++i) {
-    s.head[i] = NEG64;
-    s.tail[i] = NEG64;
-    s.support[i] = 0;
-  }
-  s.head[0] = 0;
-  s.pred_start[0] = 0;
-  s.pred_cnt[0] = 0;
-  {
-    int64_t w0 = 0;
-    for_list(J, J->in_head, J->in_cnt, J->rank_to_node[beg], [&](int, int w) { w0 += w; });
-    s.wsum[0] = w0;
-  }
-  int pc = 0;
-  for (int i = 1; i < n; ++i) {
-    const int node = J->rank_to_node[beg + i];
-    const int ps = pc;
-    bool have = false;
-    int bp = 0, bw = 0;
+// Band-guide passes of align.rs:623-680, by the whole warp. Lanes gather
+// every row's in-range predecessor list (incoming order) and successor list
+// (outgoing order) in parallel, with the total incoming weight; lane 0 then
+// runs the serial head / tail / support passes over the compact lists.
+// Predecessors whose head stays NEG are marked row = -1: the DP, the adaptive
+// update and the traceback skip them, as the reference's head filter does.
+// (head or tail, support) of the last GRING rows live in a shared-memory
+// ring so the serial passes read their neighbours without an L2 round trip.
+constexpr int GRING = 64;
+__device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int n, int64_t *ring_v,
+                                 int64_t *ring_s) {
+  const int lane = threadIdx.x & 31;
+  int pbase = 0, sbase = 0;
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    const int i = i0 + lane;
+    int cin = 0, cout = 0;
     int64_t wsum = 0;
-    for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
-      wsum += w;
-      const int r = J->rank[pred];
-      if (r < beg || r >= beg + i) return;
-      const int p = r - beg;
-      if (s.head[p] == NEG64) return;
-      s.pred[pc++] = make_int2(p, w);
-      if (!have || w > bw || (w == bw && s.support[p] > s.support[bp])) {
-        have = true;
-        bp = p;
-        bw = w;
-      }
-    });
-    s.pred_start[i] = ps;
-    s.pred_cnt[i] = pc - ps;
-    s.wsum[i] = wsum;
-    if (have) {
-      s.head[i] = s.head[bp] + 1;
-      s.support[i] = s.support[bp] + bw;
+    int node = -1;
+    if (i < n) {
+      node = J->rank_to_node[beg + i];
+      for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
+        wsum += w;
+        const int r = J->rank[pred];
+        if (r >= beg && r < beg + i) ++cin;
+      });
+      for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int) {
+        const int r = J->rank[succ];
+        if (r > beg + i && r <= end) ++cout;
+      });
     }
-  }
-  s.tail[n - 1] = 1;
-  int sc = 0;
-  s.succ_start[n - 1] = 0;
-  s.succ_cnt[n - 1] = 0;
-  {
-    // successors of the last row are outside (beg, end] by definition
-  }
-  for (int i = n - 2; i >= 0; --i) {
-    const int node = J->rank_to_node[beg + i];
-    const int ss = sc;
-    bool have = false;
-    int bs = 0, bw = 0;
-    for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int w) {
-      const int r = J->rank[succ];
-      if (r <= beg + i || r > end) return;
-      const int sx = r - beg;
-      s.succ[sc++] = sx;
-      if (s.tail[sx] == NEG64) return;
-      if (!have || w > bw || (w == bw && s.support[sx] > s.support[bs])) {
-        have = true;
-        bs = sx;
-        bw = w;
+    int pin = cin, pout = cout;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int a = __shfl_up_sync(FULL, pin, d);
+      const int b = __shfl_up_sync(FULL, pout, d);
+      if (lane >= d) {
+        pin += a;
+        pout += b;
       }
-    });
-    s.succ_start[i] = ss;
-    s.succ_cnt[i] = sc - ss;
-    if (have) {
-      s.tail[i] = s.tail[bs] + 1;
-      s.support[i] = s.support[bs] + bw;
     }
+    if (i < n) {
+      const int ps = pbase + pin - cin, ss = sbase + pout - cout;
+      s.pred_start[i] = ps;
+      s.pred_cnt[i] = cin;
+      s.succ_start[i] = ss;
+      s.succ_cnt[i] = cout;
+      s.wsum[i] = wsum;
+      int k = ps;
+      for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
+        const int r = J->rank[pred];
+        if (r >= beg && r < beg + i) s.pred[k++] = make_int2(r - beg, w);
+      });
+      k = ss;
+      for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int w) {
+        const int r = J->rank[succ];
+        if (r > beg + i && r <= end) s.succ[k++] = make_int2(r - beg, w);
+      });
+      s.head[i] = NEG64;
+      s.tail[i] = NEG64;
+      s.support[i] = 0;
+    }
+    pbase += __shfl_sync(FULL, pin, 31);
+    sbase += __shfl_sync(FULL, pout, 31);
   }
-  if (s.head[n - 1] == NEG64) return ST_NO_PATH;
-  return ST_OK;
+  __syncwarp();
+  int32_t st = ST_OK;
+  if (lane == 0) {
+    int64_t *rv = ring_v, *rs = ring_s;
+    s.head[0] = 0;
+    if (rv) {
+      rv[0] = 0;
+      rs[0] = 0;
+    }
+    for (int i = 1; i < n; ++i) {
+      bool have = false;
+      int bw = 0;
+      int64_t bsup = 0, bhead = 0;
+      const int pb = s.pred_start[i], pc = s.pred_cnt[i];
+      for (int t = 0; t < pc; ++t) {
+        const int2 e = s.pred[pb + t];
+        const bool near = rv && i - e.x < GRING;
+        const int64_t hp = near ? rv[e.x & (GRING - 1)] : s.head[e.x];
+        if (hp == NEG64) {
+          s.pred[pb + t].x = -1;
+          continue;
+        }
+        const int64_t sp = near ? rs[e.x & (GRING - 1)] : s.support[e.x];
+        if (!have || e.y > bw || (e.y == bw && sp > bsup)) {
+          have = true;
+          bw = e.y;
+          bsup = sp;
+          bhead = hp;
+        }
+      }
+      const int64_t hi = have ? bhead + 1 : NEG64;
+      const int64_t si = have ? bsup + bw : 0;
+      if (have) {
+        s.head[i] = hi;
+        s.support[i] = si;
+      }
+      if (rv) {
+        rv[i & (GRING - 1)] = hi;
+        rs[i & (GRING - 1)] = si;
+      }
+    }
+    s.tail[n - 1] = 1;
+    if (rv) rv[(n - 1) & (GRING - 1)] = 1;  // rs keeps the forward support of the last row
+    for (int i = n - 2; i >= 0; --i) {
+      bool have = false;
+      int bw = 0;
+      int64_t bsup = 0, btail = 0;
+      const int sb = s.succ_start[i], sn = s.succ_cnt[i];
+      for (int t = 0; t < sn; ++t) {
+        const int2 e = s.succ[sb + t];
+        const bool near = rv && e.x - i < GRING;
+        const int64_t ts = near ? rv[e.x & (GRING - 1)] : s.tail[e.x];
+        if (ts == NEG64) continue;
+        const int64_t ss = near ? rs[e.x & (GRING - 1)] : s.support[e.x];
+        if (!have || e.y > bw || (e.y == bw && ss > bsup)) {
+          have = true;
+          bw = e.y;
+          bsup = ss;
+          btail = ts;
+        }
+      }
+      const int64_t ti = have ? btail + 1 : NEG64;
+      const int64_t si = have ? bsup + bw : 0;
+      if (have) {
+        s.tail[i] = ti;
+        s.support[i] = si;
+      }
+      if (rv) {
+        rv[i & (GRING - 1)] = ti;
+        rs[i & (GRING - 1)] = si;
+      }
+    }
+    if (s.head[n - 1] == NEG64) st = ST_NO_PATH;
+  }
+  st = __shfl_sync(FULL, st, 0);
+  __syncwarp();
+  return st;
 }
 
 // align.rs:829-897 (lane 0): band state after row i peaked at `maximum`.
@@ -426,6 +502,7 @@ __device__ inline void adaptive_update(const Job *J, Scratch &s, int beg, int i,
   if (int(J->base[node]) == s.seq[maximum]) {
     for (int t = 0; t < s.pred_cnt[i]; ++t) {
       const int p = s.pred[s.pred_start[i] + t].x;
+      if (p < 0) continue;
       max_streak = maxs(max_streak, s.streak[p]);
       if (s.peak[p] + 1 == maximum) {
         s.streak[i] = maxs(s.streak[i], s.streak[p] + 1);
@@ -440,13 +517,13 @@ __device__ inline void adaptive_update(const Job *J, Scratch &s, int beg, int i,
     s.offset_right[i] = maximum - s.head[i];
     s.extra[i] = 0;
     for (int t = 0; t < sn; ++t) {
-      const int sx = s.succ[ss + t];
+      const int sx = s.succ[ss + t].x;
       s.offset_left[sx] = s.offset_left[i];
       s.offset_right[sx] = s.offset_right[i];
     }
   }
   for (int t = 0; t < sn; ++t) {
-    const int sx = s.succ[ss + t];
+    const int sx = s.succ[ss + t].x;
     s.offset_left[sx] = mins(s.offset_left[sx], s.offset_left[i]);
     s.offset_right[sx] = maxs(s.offset_right[sx], s.offset_right[i]);
     s.peak_left[sx] = mins(s.peak_left[sx], maximum);
@@ -501,7 +578,7 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
       const int64_t target = state == OP_MATCH ? Mv(i, j) : Dv(i, j);
       for (int t = 0; t < pc; ++t) {
         const int2 e = s.pred[pb + t];
-        if (!contains(e.x, pj)) continue;
+        if (e.x < 0 || !contains(e.x, pj)) continue;
         const int64_t source = state == OP_DELETE ? Dv(e.x, pj) : Mv(e.x, pj);
         if (target == source + penalty && (!found || e.y > bw)) {
           found = true;
@@ -599,12 +676,221 @@ __device__ inline bool i32_scores_safe(const Job *J, const DevParams &P, int beg
   return steps <= SCORE_LIMIT / P.largest;
 }
 
+// Per-warp shared memory: the M and D states of the last RING_ROWS rows,
+// indexed by absolute query column modulo RING_W, so predecessor rows are
+// read from shared memory instead of L2/HBM (a slot is valid for row r only
+// while ring_row[r % RING_ROWS] == r); the scoring matrix; the guide rings.
+constexpr int RING_ROWS = 4;
+constexpr int RING_W = 512;
+constexpr int SMEM_MATRIX = 512;  // sigma^2 entries kept in shared memory (sigma <= 22)
+struct WarpSmem {
+  int32_t ring_m[RING_ROWS][RING_W];
+  int32_t ring_d[RING_ROWS][RING_W];
+  int32_t ring_row[RING_ROWS];
+  int32_t matrix[SMEM_MATRIX];
+  int64_t gring_v[GRING];  // guide passes: head (forward) or tail (backward)
+  int64_t gring_s[GRING];  // guide passes: support
+};
+
+// One int32 DP row of at most 32*C columns (align.rs:751-828) as a blocked
+// register tile: lane l owns columns [start + C*l, start + C*l + C). The
+// predecessors (band, arena row and ring slot held by the lanes of `vmask`)
+// are folded into M and D; each lane scans its block serially, one warp
+// max-plus scan over the lane aggregates (shift C*E per lane) gives every
+// lane its carried-in insertion state, and a per-lane fixup finishes I and
+// M. All identities are exact in integers: I[j+1] = max(I[j] + E, md[j] + O)
+// with I[start] = NEG32.
+template <int C>
+__device__ __forceinline__ void dp_row_blocked(int lane, int start, int len, int32_t *R, const int32_t *seq,
+                                               const int32_t *mrow, int32_t E, int32_t O, unsigned vmask,
+                                               int my_ps, int my_pl, int my_slot, const int32_t *my_g,
+                                               WarpSmem *sm, int out_slot, bool adapt, int32_t &bestv,
+                                               int &bestj) {
+  const int stop = start + len;
+  const int j0 = start + C * lane;
+  int32_t Mx[C], Dx[C];
+#pragma unroll
+  for (int k = 0; k < C; ++k) {
+    Mx[k] = NEG32;
+    Dx[k] = NEG32;
+  }
+  while (vmask) {
+    const int t = __ffs(vmask) - 1;
+    vmask &= vmask - 1;
+    const int ps = __shfl_sync(FULL, my_ps, t);
+    const int pl = __shfl_sync(FULL, my_pl, t);
+    const int slot = __shfl_sync(FULL, my_slot, t);
+    const int32_t *g = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
+    if (slot >= 0) {
+      const int32_t *rm = sm->ring_m[slot];
+      const int32_t *rd = sm->ring_d[slot];
+      int32_t prev = (j0 > ps && j0 - 1 < ps + pl) ? rm[(j0 - 1) & (RING_W - 1)] : NEG32;
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        const int j = j0 + k;
+        const bool in = unsigned(j - ps) < unsigned(pl);
+        const int32_t mp = rm[j & (RING_W - 1)], dp = rd[j & (RING_W - 1)];
+        if (in) {
+          Mx[k] = maxs(Mx[k], prev);
+          Dx[k] = maxs(Dx[k], maxs(dp + E, mp + O));
+        }
+        prev = in ? mp : NEG32;
+      }
+    } else {
+      int32_t prev = (j0 > ps && j0 - 1 < ps + pl) ? g[j0 - 1 - ps] : NEG32;
+#pragma unroll
+      for (int k = 0; k < C; ++k) {
+        const int j = j0 + k;
+        const bool in = unsigned(j - ps) < unsigned(pl);
+        int32_t mp = NEG32, dp = NEG32;
+        if (in) {
+          mp = g[j - ps];
+          dp = g[pl + j - ps];
+          Mx[k] = maxs(Mx[k], prev);
+          Dx[k] = maxs(Dx[k], maxs(dp + E, mp + O));
+        }
+        prev = mp;
+      }
+    }
+  }
+  // md and the in-block scan x[k] = max over k' <= k of md[k'] + O + (k-k')E
+  int32_t X[C];
+#pragma unroll
+  for (int k = 0; k < C; ++k) {
+    const int j = j0 + k;
+    const int32_t prof = j < stop ? mrow[seq[j]] : 0;
+    Mx[k] = maxs(Mx[k] + prof, Dx[k]);  // Mx now holds md
+    X[k] = Mx[k] + O;
+    if (k > 0) X[k] = maxs(X[k], X[k - 1] + E);
+  }
+  // lane aggregates: y_l = max over k < start + C(l+1) of md[k] + O + shift
+  int32_t y = X[C - 1];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int32_t v = __shfl_up_sync(FULL, y, d);
+    if (lane >= d) y = maxs(y, v + d * C * E);
+  }
+  int32_t cin = __shfl_up_sync(FULL, y, 1);
+  cin = lane == 0 ? NEG32 : maxs(cin, NEG32 + C * lane * E);
+  __syncwarp();  // every predecessor read of the ring precedes this row's writes
+  if (j0 < stop) {
+    const int o = C * lane;
+#pragma unroll
+    for (int k0 = 0; k0 < C; k0 += 4) {
+      if (j0 + k0 < stop) {
+        int32_t iv[4], mv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int k = k0 + q;
+          iv[q] = k == 0 ? cin : maxs(X[k - 1], cin + k * E);
+          mv[q] = maxs(Mx[k], iv[q]);
+          const int j = j0 + k;
+          sm->ring_m[out_slot][j & (RING_W - 1)] = mv[q];
+          sm->ring_d[out_slot][j & (RING_W - 1)] = Dx[k];
+          if (adapt && mv[q] > bestv) {
+            bestv = mv[q];
+            bestj = j;
+          }
+        }
+        *reinterpret_cast<int4 *>(R + o + k0) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+        *reinterpret_cast<int4 *>(R + len + o + k0) = make_int4(Dx[k0], Dx[k0 + 1], Dx[k0 + 2], Dx[k0 + 3]);
+        *reinterpret_cast<int4 *>(R + 2 * len + o + k0) = make_int4(iv[0], iv[1], iv[2], iv[3]);
+      }
+    }
+  }
+}
+
+// Dispatches one int32 row to the blocked tile of the right width.
+__device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_t *R, const int32_t *seq,
+                                            const int32_t *mrow, int32_t E, int32_t O, unsigned vmask, int ps,
+                                            int pl, int slot, const int32_t *g, WarpSmem *sm, int out_slot,
+                                            bool adapt, int32_t &bv, int &bj) {
+  if (len <= 128)
+    dp_row_blocked<4>(lane, start, len, R, seq, mrow, E, O, vmask, ps, pl, slot, g, sm, out_slot, adapt, bv, bj);
+  else if (len <= 256)
+    dp_row_blocked<8>(lane, start, len, R, seq, mrow, E, O, vmask, ps, pl, slot, g, sm, out_slot, adapt, bv, bj);
+  else
+    dp_row_blocked<16>(lane, start, len, R, seq, mrow, E, O, vmask, ps, pl, slot, g, sm, out_slot, adapt, bv, bj);
+}
+
+// One row by the generic interleaved loop (int64 kernel, rows wider than
+// RING_W, or more than 32 predecessors): 32-column chunks, predecessor rows
+// from the arena, a warp-shuffle scan per chunk with a serial carry.
+template <typename S>
+__device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *R, const S *A, const Scratch &s,
+                                               int pb, int pc, const int32_t *mrow, S E, S O, bool adapt, S &bestv,
+                                               int &bestj) {
+  constexpr S NEGV = ScoreTraits<S>::NEGV;
+  const int stop = start + len;
+  S carry = NEGV;
+  for (int c0 = start; c0 < stop; c0 += 32) {
+    const int j = c0 + lane;
+    const bool valid = j < stop;
+    S M = NEGV, D = NEGV;
+    if (valid) {
+      for (int t = 0; t < pc; ++t) {
+        const int p = s.pred[pb + t].x;
+        if (p < 0) continue;
+        const int ps = s.row_start[p], pl = s.row_len[p];
+        if (j >= ps && j < ps + pl) {
+          const S *Q = A + s.row_off[p];
+          const int k = j - ps;
+          const S mp = Q[k], dp = Q[pl + k];
+          const S dg = k > 0 ? Q[k - 1] : NEGV;
+          M = maxs(M, dg);
+          D = maxs(D, maxs<S>(dp + E, mp + O));
+        }
+      }
+    }
+    const S prof = valid ? S(mrow[s.seq[j]]) : S(0);
+    const S md = maxs<S>(M + prof, D);
+    S x = md + O;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const S y = shfl_up_s(x, d);
+      if (lane >= d) x = maxs<S>(x, y + S(d) * E);
+    }
+    x = maxs<S>(x, carry + S(lane + 1) * E);
+    S I = shfl_up_s(x, 1);
+    if (lane == 0) I = carry;
+    const S Mf = maxs(md, I);
+    if (valid) {
+      const int c = j - start;
+      R[c] = Mf;
+      R[len + c] = D;
+      R[2 * len + c] = I;
+      if (adapt && Mf > bestv) {
+        bestv = Mf;
+        bestj = j;
+      }
+    }
+    carry = shfl_s(x, 31);
+  }
+}
+
+// Row 0 (align.rs:737-750), serial on lane 0.
+template <typename S>
+__device__ __forceinline__ void dp_row0(S *R, int len, S s00, S E, S O) {
+  constexpr S NEGV = ScoreTraits<S>::NEGV;
+  for (int c = 0; c < len; ++c) {
+    R[c] = NEGV;
+    R[len + c] = NEGV;
+  }
+  R[0] = s00;
+  R[2 * len] = NEGV;
+  for (int c = 1; c < len; ++c) {
+    const S ins = maxs<S>(R[2 * len + c - 1] + E, R[c - 1] + O);
+    R[2 * len + c] = ins;
+    R[c] = maxs<S>(R[c], ins);
+  }
+}
+
 // One DP kernel invocation (poa_simd_arena, align.rs:588-911, or
 // poa_scalar_i64, align.rs:913-1162) by a whole warp.
 template <typename S>
 __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t arena_bytes, int beg_id, int end_id,
                               const uint8_t *query, int qlen, bool adaptive_arg, uint64_t band_b, uint64_t f,
-                              Scratch &s, int *n_items, Work *cells) {
+                              Scratch &s, int *n_items, Work *cells, WarpSmem *sm) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
   const int lane = threadIdx.x & 31;
   if (beg_id >= J->n_nodes || end_id >= J->n_nodes) return ST_ANCHOR_NOT_IN_GRAPH;
@@ -622,133 +908,253 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   if (bandu < band_b) bandu = UINT64_MAX;
   const int64_t band = int64_t(bandu < uint64_t(INT32_MAX) ? bandu : uint64_t(INT32_MAX));
   const S E = S(P.gap_ext), O = S(P.gap_open);
-  int32_t st = ST_OK;
+  const S s00 = S(P.matrix[P.unknown * P.sigma + P.unknown]);
   __syncwarp();
-  if (lane == 0) st = guides(J, s, beg, end, n);
-  st = __shfl_sync(FULL, st, 0);
+  int32_t st = guides(J, s, beg, end, n, sm ? sm->gring_v : nullptr, sm ? sm->gring_s : nullptr);
   if (st != ST_OK) return st;
-  for (int i = lane; i < n; i += 32) {
-    s.peak[i] = 0;
-    s.streak[i] = 0;
-    s.peak_left[i] = m;
-    s.peak_right[i] = 0;
-    s.offset_left[i] = 0;
-    s.offset_right[i] = 0;
-    s.extra[i] = 0;
+  const bool do_adapt = f != 0 && adaptive;
+  if (do_adapt) {
+    for (int i = lane; i < n; i += 32) {
+      s.peak[i] = 0;
+      s.streak[i] = 0;
+      s.peak_left[i] = m;
+      s.peak_right[i] = 0;
+      s.offset_left[i] = 0;
+      s.offset_right[i] = 0;
+      s.extra[i] = 0;
+    }
   }
-  __syncwarp();
   S *A = reinterpret_cast<S *>(s.dp);
   const int64_t cap = s.dp_bytes / int64_t(sizeof(S));
-  int64_t cursor = 0;
   uint64_t row_cells = 0;
-  const bool do_adapt = f != 0 && adaptive;
-  for (int i = 0; i < n; ++i) {
-    const int64_t hi = s.head[i], ti = s.tail[i];
-    if (hi == NEG64 || ti == NEG64) {
-      if (lane == 0) {
-        s.row_start[i] = 0;
-        s.row_len[i] = 0;
-        s.row_off[i] = 0;
-      }
-      __syncwarp();
-      continue;
-    }
-    int64_t left, right;
-    if (f == 0) {
-      left = 0;
-      right = m;
-    } else if (adaptive) {
-      const int64_t x = mins(mins(s.peak_left[i], hi + s.offset_left[i]), m - ti);
-      const int64_t y = maxs(maxs(s.peak_right[i], hi + s.offset_right[i]), m - ti);
-      left = maxs<int64_t>(x - band - s.extra[i], 0);
-      right = mins<int64_t>(y + band + s.extra[i], m);
-    } else {
-      left = maxs<int64_t>(mins(hi, m - ti) - band, 0);
-      right = mins<int64_t>(maxs(hi, m - ti) + band, m);
-    }
-    if (left > right || right < 0) return ST_BAND_NO_INTERSECT;
-    const int start = int(left / 8 * 8);
-    const int stop = int((right / 8 + 1) * 8);
-    const int len = stop - start;
-    if (cursor + 3 * int64_t(len) > cap) return ST_ARENA_FULL;
-    const int64_t off = cursor;
-    cursor += 3 * int64_t(len);
-    row_cells += uint64_t(len);
-    if (lane == 0) {
-      s.row_start[i] = start;
-      s.row_len[i] = len;
-      s.row_off[i] = off;
-    }
-    S *R = A + off;
-    if (i == 0) {
-      if (start != 0) return ST_BAND_EXCLUDES_SOURCE;
-      if (lane == 0) {
-        for (int c = 0; c < len; ++c) {
-          R[c] = NEGV;
-          R[len + c] = NEGV;
-        }
-        R[0] = S(P.matrix[P.unknown * P.sigma + P.unknown]);
-        R[2 * len] = NEGV;
-        for (int c = 1; c < len; ++c) {
-          const S ins = maxs<S>(R[2 * len + c - 1] + E, R[c - 1] + O);
-          R[2 * len + c] = ins;
-          R[c] = maxs<S>(R[c], ins);
-        }
-      }
-      __syncwarp();
-      continue;
-    }
-    const int node = J->rank_to_node[beg + i];
-    const int base = (i == n - 1) ? P.unknown : int(J->base[node]);
-    const int32_t *mrow = P.matrix + base * P.sigma;
-    const int pb = s.pred_start[i], pc = s.pred_cnt[i];
-    S carry = NEGV;
-    S bestv = ScoreTraits<S>::LOWEST;
-    int bestj = INT32_MAX;
-    for (int c0 = start; c0 < stop; c0 += 32) {
-      const int j = c0 + lane;
-      const bool valid = j < stop;
-      S M = NEGV, D = NEGV;
-      if (valid) {
-        for (int t = 0; t < pc; ++t) {
-          const int p = s.pred[pb + t].x;
-          const int ps = s.row_start[p], pl = s.row_len[p];
-          if (j >= ps && j < ps + pl) {
-            const S *Q = A + s.row_off[p];
-            const int k = j - ps;
-            const S mp = Q[k], dp = Q[pl + k];
-            const S dg = k > 0 ? Q[k - 1] : NEGV;
-            M = maxs(M, dg);
-            D = maxs(D, maxs<S>(dp + E, mp + O));
+  constexpr bool kFastType = sizeof(S) == 4;
+  const bool smem_matrix = P.sigma * P.sigma <= SMEM_MATRIX;
+  if (sm) {
+    if (lane < RING_ROWS) sm->ring_row[lane] = -1;
+    if (smem_matrix)
+      for (int k = lane; k < P.sigma * P.sigma; k += 32) sm->matrix[k] = P.matrix[k];
+  }
+  __syncwarp();
+  if (!do_adapt) {
+    // Static band (align.rs:711-734 with f == 0 or without adaptive band):
+    // every row's band is fixed once the guides are known, so the warp plans
+    // all rows at once (band, base code, arena offset). The first failing row
+    // in row order gives the reference's status.
+    int64_t tot = 0;
+    int err_code = ST_OK;
+    uint64_t err_cells = 0;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+      const int i = i0 + lane;
+      int start = 0, len = 0, code = ST_OK;
+      if (i < n) {
+        const int64_t hi = s.head[i], ti = s.tail[i];
+        if (hi != NEG64 && ti != NEG64) {
+          int64_t left, right;
+          if (f == 0) {
+            left = 0;
+            right = m;
+          } else {
+            left = maxs<int64_t>(mins(hi, m - ti) - band, 0);
+            right = mins<int64_t>(maxs(hi, m - ti) + band, m);
+          }
+          if (left > right || right < 0) {
+            code = ST_BAND_NO_INTERSECT;
+          } else {
+            start = int(left / 8 * 8);
+            len = int((right / 8 + 1) * 8) - start;
+            if (i == 0 && start != 0) code = ST_BAND_EXCLUDES_SOURCE;
           }
         }
+        s.row_base[i] = (i == n - 1) ? P.unknown : int(J->base[J->rank_to_node[beg + i]]);
       }
-      const S prof = valid ? S(mrow[s.seq[j]]) : S(0);
-      const S md = maxs<S>(M + prof, D);
-      S x = md + O;
+      const int64_t own = 3 * int64_t(len);
+      int64_t inc = own;
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
-        const S y = shfl_up_s(x, d);
-        if (lane >= d) x = maxs<S>(x, y + S(d) * E);
+        const int64_t v = shfl_up_s(inc, d);
+        if (lane >= d) inc += v;
       }
-      x = maxs<S>(x, carry + S(lane + 1) * E);
-      S I = shfl_up_s(x, 1);
-      if (lane == 0) I = carry;
-      const S Mf = maxs(md, I);
-      if (valid) {
-        const int c = j - start;
-        R[c] = Mf;
-        R[len + c] = D;
-        R[2 * len + c] = I;
-        if (Mf > bestv) {
-          bestv = Mf;
-          bestj = j;
-        }
+      if (i < n) {
+        s.row_start[i] = start;
+        s.row_len[i] = len;
+        s.row_off[i] = tot + inc - own;
       }
-      carry = shfl_s(x, 31);
+      const unsigned bad = __ballot_sync(FULL, code != ST_OK);
+      if (bad && err_code == ST_OK) {
+        const int l = __ffs(bad) - 1;
+        err_code = __shfl_sync(FULL, code, l);
+        // rows the reference allocates before it stops (row 0 is allocated
+        // before its source check)
+        const int64_t before = shfl_s(int64_t(inc - own), l) / 3;
+        const int flen = __shfl_sync(FULL, len, l);
+        err_cells = row_cells + uint64_t(before) + (err_code == ST_BAND_EXCLUDES_SOURCE ? uint64_t(flen) : 0);
+      }
+      const int64_t group = shfl_s(inc, 31);
+      row_cells += uint64_t(group / 3);
+      tot += group;
+    }
+    if (err_code != ST_OK) {
+      cells->cells += err_cells;
+      cells->dp_bytes += err_cells * 3 * sizeof(S);
+      return err_code;
+    }
+    if (tot > cap) return ST_ARENA_FULL;
+    __syncwarp();
+    const int etot = s.pred_start[n - 1] + s.pred_cnt[n - 1];
+    for (int e = lane; e < etot; e += 32) {
+      const int p = s.pred[e].x;
+      if (p >= 0) {
+        s.pmeta[e] = make_int4(p, s.row_start[p], s.row_len[p], 0);
+        s.pmeta_off[e] = s.row_off[p];
+      } else {
+        s.pmeta[e] = make_int4(-1, 0, 0, 0);
+        s.pmeta_off[e] = 0;
+      }
     }
     __syncwarp();
-    if (do_adapt) {
+    if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
+    __syncwarp();
+    // rows 1..n-1, software-pipelined: row i+2's descriptor and row i+1's
+    // predecessor metadata are loaded while row i computes
+    auto desc = [&](int r) { return make_int4(s.row_start[r], s.row_len[r], s.pred_start[r], s.pred_cnt[r]); };
+    int4 d1 = n > 1 ? desc(1) : make_int4(0, 0, 0, 0);
+    int4 d2 = n > 2 ? desc(2) : make_int4(0, 0, 0, 0);
+    int64_t o1 = n > 1 ? s.row_off[1] : 0, o2 = n > 2 ? s.row_off[2] : 0;
+    int b1 = n > 1 ? s.row_base[1] : 0, b2 = n > 2 ? s.row_base[2] : 0;
+    int4 m1 = make_int4(-1, 0, 0, 0);
+    int64_t mo1 = 0;
+    if (n > 1 && lane < d1.w) {
+      m1 = s.pmeta[d1.z + lane];
+      mo1 = s.pmeta_off[d1.z + lane];
+    }
+    for (int i = 1; i < n; ++i) {
+      const int4 d = d1;
+      const int64_t off = o1;
+      const int base = b1;
+      const int4 mt = m1;
+      const int64_t mo = mo1;
+      d1 = d2;
+      o1 = o2;
+      b1 = b2;
+      m1 = make_int4(-1, 0, 0, 0);
+      mo1 = 0;
+      if (i + 1 < n && lane < d1.w) {
+        m1 = s.pmeta[d1.z + lane];
+        mo1 = s.pmeta_off[d1.z + lane];
+      }
+      if (i + 2 < n) {
+        d2 = desc(i + 2);
+        o2 = s.row_off[i + 2];
+        b2 = s.row_base[i + 2];
+      }
+      const int start = d.x, len = d.y, pb = d.z, pc = d.w;
+      if (len == 0) continue;
+      S *R = A + off;
+      if (kFastType && sm && len <= RING_W && pc <= 32) {
+        const int p = mt.x;
+        const bool ok = p >= 0 && mt.z > 0;
+        const int sl = p >= 0 ? p % RING_ROWS : 0;
+        const int my_slot = (ok && sm->ring_row[sl] == p) ? sl : -1;
+        const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + mo;
+        const unsigned vmask = __ballot_sync(FULL, ok);
+        const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
+        int32_t bv = INT32_MIN;
+        int bj = INT32_MAX;
+        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), s.seq, mrow, int32_t(E), int32_t(O), vmask,
+                    mt.y, mt.z, my_slot, my_g, sm, i % RING_ROWS, false, bv, bj);
+        __syncwarp();
+        if (lane == 0) sm->ring_row[i % RING_ROWS] = i;
+        __syncwarp();
+        continue;
+      }
+      if (sm && lane == 0) sm->ring_row[i % RING_ROWS] = -1;
+      S bv = ScoreTraits<S>::LOWEST;
+      int bj = INT32_MAX;
+      dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, false, bv, bj);
+      __syncwarp();
+    }
+  } else {
+    // Adaptive band (align.rs:711-729, 829-897): row i's band follows its
+    // predecessors' peaks, so rows are planned one at a time.
+    int64_t cursor = 0;
+    for (int i = 0; i < n; ++i) {
+      const int64_t hi = s.head[i], ti = s.tail[i];
+      if (hi == NEG64 || ti == NEG64) {
+        if (lane == 0) {
+          s.row_start[i] = 0;
+          s.row_len[i] = 0;
+          s.row_off[i] = 0;
+        }
+        __syncwarp();
+        continue;
+      }
+      const int64_t x = mins(mins(s.peak_left[i], hi + s.offset_left[i]), m - ti);
+      const int64_t y = maxs(maxs(s.peak_right[i], hi + s.offset_right[i]), m - ti);
+      const int64_t left = maxs<int64_t>(x - band - s.extra[i], 0);
+      const int64_t right = mins<int64_t>(y + band + s.extra[i], m);
+      if (left > right || right < 0) {
+        cells->cells += row_cells;
+        cells->dp_bytes += row_cells * 3 * sizeof(S);
+        return ST_BAND_NO_INTERSECT;
+      }
+      const int start = int(left / 8 * 8);
+      const int stop = int((right / 8 + 1) * 8);
+      const int len = stop - start;
+      if (cursor + 3 * int64_t(len) > cap) return ST_ARENA_FULL;
+      const int64_t off = cursor;
+      cursor += 3 * int64_t(len);
+      row_cells += uint64_t(len);
+      if (lane == 0) {
+        s.row_start[i] = start;
+        s.row_len[i] = len;
+        s.row_off[i] = off;
+      }
+      S *R = A + off;
+      if (i == 0) {
+        if (start != 0) {
+          cells->cells += row_cells;
+          cells->dp_bytes += row_cells * 3 * sizeof(S);
+          return ST_BAND_EXCLUDES_SOURCE;
+        }
+        if (lane == 0) dp_row0<S>(R, len, s00, E, O);
+        __syncwarp();
+        continue;
+      }
+      const int node = J->rank_to_node[beg + i];
+      const int base = (i == n - 1) ? P.unknown : int(J->base[node]);
+      const int pb = s.pred_start[i], pc = s.pred_cnt[i];
+      S bestv = ScoreTraits<S>::LOWEST;
+      int bestj = INT32_MAX;
+      if (kFastType && sm && len <= RING_W && pc <= 32) {
+        int my_ps = 0, my_pl = 0, my_slot = -1;
+        const int32_t *my_g = nullptr;
+        bool ok = false;
+        if (lane < pc) {
+          const int p = s.pred[pb + lane].x;
+          if (p >= 0) {
+            my_ps = s.row_start[p];
+            my_pl = s.row_len[p];
+            my_g = reinterpret_cast<const int32_t *>(A) + s.row_off[p];
+            const int sl = p % RING_ROWS;
+            my_slot = sm->ring_row[sl] == p ? sl : -1;
+            ok = my_pl > 0;
+          }
+        }
+        const unsigned vmask = __ballot_sync(FULL, ok);
+        const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
+        int32_t bv = INT32_MIN;
+        int bj = INT32_MAX;
+        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), s.seq, mrow, int32_t(E), int32_t(O), vmask,
+                    my_ps, my_pl, my_slot, my_g, sm, i % RING_ROWS, true, bv, bj);
+        __syncwarp();
+        if (lane == 0) sm->ring_row[i % RING_ROWS] = i;
+        bestv = S(bv);
+        bestj = bj;
+      } else {
+        if (sm && lane == 0) sm->ring_row[i % RING_ROWS] = -1;
+        dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, true, bestv, bestj);
+      }
+      __syncwarp();
       S v = bestv;
       int jj = bestj;
 #pragma unroll
@@ -775,27 +1181,29 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
 // poa_inner (align.rs:531-545): score-guard dispatch.
 __device__ inline int32_t poa_inner(Job *J, const DevParams &P, char *arena, int64_t bytes, int beg_id, int end_id,
                                     const uint8_t *q, int qlen, bool adaptive, uint64_t band_b, uint64_t f,
-                                    Scratch &s, int *n_items, Work *cells) {
+                                    Scratch &s, int *n_items, Work *cells, WarpSmem *sm) {
   const bool use32 = P.kernel == 1 || (P.kernel == 0 && i32_scores_safe(J, P, beg_id, end_id, qlen));
   if (use32)
-    return poa_kernel<int32_t>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells);
-  return poa_kernel<int64_t>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells);
+    return poa_kernel<int32_t>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells,
+                               sm);
+  return poa_kernel<int64_t>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells,
+                             sm);
 }
 
 // poa (align.rs:192-211): on an alignment error with f != 0, retry with the
 // full matrix (f = 0, static band).
 __device__ inline int32_t poa_retry(Job *J, const DevParams &P, char *arena, int64_t bytes, int beg_id, int end_id,
                                     const uint8_t *q, int qlen, bool adaptive, uint64_t band_b, Scratch &s,
-                                    int *n_items, Work *cells) {
-  int32_t st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, P.f, s, n_items, cells);
+                                    int *n_items, Work *cells, WarpSmem *sm) {
+  int32_t st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, P.f, s, n_items, cells, sm);
   if (is_alignment_error(st) && P.f != 0)
-    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, false, band_b, 0, s, n_items, cells);
+    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, false, band_b, 0, s, n_items, cells, sm);
   return st;
 }
 
 // align::align (align.rs:81-98) for unseeded parameters; writes s.items.
 __device__ inline int32_t align_query(Job *J, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q,
-                                      int qlen, Scratch &s, int *n_items, Work *cells) {
+                                      int qlen, Scratch &s, int *n_items, Work *cells, WarpSmem *sm) {
   const int lane = threadIdx.x & 31;
   if (J->n_nodes <= 2) {
     if (!carve_scratch(arena, bytes, 2, 0, (int64_t(qlen) + 2) / 8 * 8 + 8, int64_t(qlen) + 3, s))
@@ -807,13 +1215,109 @@ __device__ inline int32_t align_query(Job *J, const DevParams &P, char *arena, i
     return ST_OK;
   }
   if (P.seeding) return ST_SEEDING_UNSUPPORTED;
-  return poa_retry(J, P, arena, bytes, 0, 1, q, qlen, P.adaptive != 0, P.b, s, n_items, cells);
+  return poa_retry(J, P, arena, bytes, 0, 1, q, qlen, P.adaptive != 0, P.b, s, n_items, cells, sm);
+}
+
+// Splices a read's new nodes into the current topological order (warp-wide):
+// each run of consecutive new nodes on the path is placed right after the
+// pre-existing path node before it. The result is a valid topological order
+// when consecutive pre-existing path nodes keep increasing ranks; otherwise
+// nothing is changed and false is returned (the caller then runs the LIFO
+// toposort of graph.rs:125-178). With a static band and no seeding the rank
+// order does not change any alignment: band guides, DP states and traceback
+// choices depend only on the predecessor / successor lists in insertion order.
+__device__ inline bool reorder_incremental(Job *J, const int4 *items, int n_items, int n_old, char *buf,
+                                           int64_t buf_bytes) {
+  const int lane = threadIdx.x & 31;
+  const int n_new = J->n_nodes;
+  if (J->n_rank != n_old || n_items <= 0) return false;
+  if (int64_t(4) * (2 * int64_t(n_old) + n_new) > buf_bytes) return false;
+  int32_t *add = reinterpret_cast<int32_t *>(buf);
+  int32_t *first = add + n_old;
+  int32_t *nr2n = first + n_old;
+  for (int r = lane; r < n_old; r += 32) add[r] = 0;
+  __syncwarp();
+  long long carry = -1;  // last pre-existing path item as (index << 32 | rank)
+  bool bad = false;
+  for (int t0 = 0; t0 < n_items; t0 += 32) {
+    const int t = t0 + lane;
+    const int id = t < n_items ? items[t].w : -1;
+    const bool old = t < n_items && id >= 0 && id < n_old;
+    const int rk = old ? J->rank[id] : 0;
+    long long inc = old ? ((long long)t << 32) | (unsigned)rk : -1;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const long long v = __shfl_up_sync(FULL, inc, d);
+      if (lane >= d) inc = inc > v ? inc : v;
+    }
+    long long prev = __shfl_up_sync(FULL, inc, 1);
+    if (lane == 0) prev = -1;
+    prev = prev > carry ? prev : carry;
+    if (old && prev >= 0) {
+      const int pt = int(prev >> 32), pr = int(prev & 0xffffffffLL);
+      if (pr >= rk) bad = true;
+      if (t - pt - 1 > 0) {
+        add[pr] = t - pt - 1;
+        first[pr] = items[pt + 1].w;
+      }
+    }
+    const long long last = __shfl_sync(FULL, inc, 31);
+    carry = last > carry ? last : carry;
+  }
+  if (__any_sync(FULL, bad) || carry < 0) return false;
+  if (lane == 0) {
+    const int pt = int(carry >> 32), pr = int(carry & 0xffffffffLL);
+    if (n_items - pt - 1 > 0) {
+      add[pr] = n_items - pt - 1;
+      first[pr] = items[pt + 1].w;
+    }
+  }
+  __syncwarp();
+  int shift = 0;
+  for (int r0 = 0; r0 < n_old; r0 += 32) {
+    const int r = r0 + lane;
+    const int a = r < n_old ? add[r] : 0;
+    int inc = a;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(FULL, inc, d);
+      if (lane >= d) inc += v;
+    }
+    if (r < n_old) {
+      const int node = J->rank_to_node[r];
+      const int nr = r + shift + inc - a;
+      nr2n[nr] = node;
+      J->rank[node] = nr;
+      for (int k = 0; k < a; ++k) {
+        const int id = first[r] + k;
+        nr2n[nr + 1 + k] = id;
+        J->rank[id] = nr + 1 + k;
+      }
+    }
+    shift += __shfl_sync(FULL, inc, 31);
+  }
+  __syncwarp();
+  for (int r = lane; r < n_new; r += 32) J->rank_to_node[r] = nr2n[r];
+  if (lane == 0) J->n_rank = n_new;
+  __syncwarp();
+  return true;
+}
+
+// The exact LIFO order (graph.rs:125-178) when the current one came from
+// reorder_incremental (lane 0; the arena holds the degree and stack arrays).
+__device__ inline int32_t finalize_order(Job *J, char *arena, int64_t bytes) {
+  if (J->order_exact) return ST_OK;
+  if (int64_t(J->n_nodes) * 8 > bytes) return ST_ARENA_FULL;
+  int32_t *deg = reinterpret_cast<int32_t *>(arena);
+  const int32_t st = toposort(J, deg, deg + J->n_nodes);
+  if (st == ST_OK) J->order_exact = 1;
+  return st;
 }
 
 // One step of extend_graph (lib.rs:199-201): align, add_path, toposort(false).
 // Capacity is checked before the DP so a full graph stops cleanly.
 __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q,
-                                     int qlen, int r) {
+                                     int qlen, int r, WarpSmem *sm) {
   const int lane = threadIdx.x & 31;
   if (J->n_nodes + qlen + 2 > J->node_cap || J->n_chunks + 2 * (qlen + 3) > J->chunk_cap ||
       J->path_used + qlen + 1 > J->path_cap || J->n_paths + 1 > J->max_paths)
@@ -825,16 +1329,28 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   Scratch s;
   int n_items = 0;
   Work cells{};
-  int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells);
+  int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, sm);
   if (st != ST_OK) return st;
+  const int n_old = J->n_nodes;
+  if (lane == 0) st = add_path(J, P, r, s.items, n_items);
+  st = __shfl_sync(FULL, st, 0);
+  __syncwarp();
+  if (st != ST_OK) return st;
+  // order-free reads (static band, no seeding) keep a spliced order; the
+  // others, and any splice that would break the order, use the LIFO toposort
+  const bool order_free = P.relaxed_order && !P.seeding && !(P.adaptive && P.f != 0);
+  bool spliced = false;
+  if (order_free) spliced = reorder_incremental(J, s.items, n_items, n_old, s.dp, s.dp_bytes);
   if (lane == 0) {
-    // toposort runs after add_path has consumed s.items, so its scratch may
-    // overwrite the front of the arena.
-    st = add_path(J, P, r, s.items, n_items);
-    if (st == ST_OK) {
+    if (spliced) {
+      J->order_exact = 0;
+    } else {
+      // toposort runs after add_path has consumed s.items, so its scratch may
+      // overwrite the front of the arena.
       int32_t *deg = reinterpret_cast<int32_t *>(arena);
       int32_t *stack = deg + nodes_after;
       st = toposort(J, deg, stack);
+      J->order_exact = 1;
     }
     if (st == ST_OK) {
       J->cells += cells.cells;

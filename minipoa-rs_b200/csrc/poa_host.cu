@@ -240,6 +240,7 @@ struct poa_ctx {
     P.adaptive = hp.adaptive ? 1 : 0;
     P.kernel = 0;
     P.seeding = hp.seeding ? 1 : 0;
+    P.relaxed_order = 1;  // read loops finish with the exact LIFO order
     P.b = hp.b;
     P.f = hp.f;
     P.largest = hp.largest();

@@ -19,7 +19,7 @@ cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, i
 cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q, int qlen,
                          int mode, int beg_id, int end_id, int adaptive, uint64_t band_b, int retry, int4 *out,
                          int32_t *out_n, cudaStream_t stream);
-cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, const int4 *items, int n,
+cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, int4 *items, int n,
                             cudaStream_t stream);
 cudaError_t launch_add_node(Job *job_dev, int sigma, int base, cudaStream_t stream);
 cudaError_t launch_add_edge(Job *job_dev, int from, int to, cudaStream_t stream);

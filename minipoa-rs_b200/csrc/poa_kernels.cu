@@ -1,23 +1,31 @@
 // Kernels of the B200 POA library: the persistent batched read-loop kernel,
 // the plain one-read-per-launch kernel, and the single-graph operations behind
 // the reference-shaped C ABI. One warp per job; blocks of WARPS_PER_BLOCK
-// independent warps.
+// independent warps, each with its own slice of dynamic shared memory.
 #include "poa_internal.h"
 
 namespace poa {
 
 constexpr int WARPS_PER_BLOCK = 4;
 
+__device__ __forceinline__ WarpSmem *warp_smem() {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  return reinterpret_cast<WarpSmem *>(dyn_smem) + (threadIdx.x >> 5);
+}
+
 // Persistent batched kernel: each warp takes jobs from a size-ordered queue
 // (largest first) and runs their remaining reads. A job that outgrows the
 // warp's DP arena parks at its current read (graph untouched) for a later
 // pass with larger arenas.
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3)
     k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *queue, DevParams P, char *arenas,
-            int64_t slot_bytes) {
+            int64_t slot_bytes, int slots) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  // the grid is rounded up to whole blocks; warps past the last slot own no arena
+  if (warp >= slots) return;
   char *arena = arenas + warp * slot_bytes;
+  WarpSmem *sm = warp_smem();
   for (;;) {
     int q = 0;
     if (lane == 0) q = atomicAdd(queue, 1);
@@ -25,12 +33,19 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
     if (q >= n_jobs) break;
     Job *J = jobs + order[q];
     const int n_reads = J->n_reads;
+    int32_t st = ST_OK;
     for (int r = J->next_read; r < n_reads; ++r) {
-      const int32_t st = extend_one(J, P, arena, slot_bytes, J->reads + J->read_off[r], J->read_len[r], r);
-      if (st != ST_OK) {
-        if (lane == 0) J->status = st;
-        break;
+      st = extend_one(J, P, arena, slot_bytes, J->reads + J->read_off[r], J->read_len[r], r, sm);
+      if (st != ST_OK) break;
+    }
+    // a finished (or failed) job ends with the reference's exact rank order;
+    // a parked job keeps its order for the next pass
+    if (lane == 0) {
+      if (st == ST_OK || is_alignment_error(st)) {
+        const int32_t fs = finalize_order(J, arena, slot_bytes);
+        if (st == ST_OK) st = fs;
       }
+      J->status = st;
     }
     __syncwarp();
   }
@@ -39,19 +54,30 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32)
 // Plain form: one launch aligns one read of one job.
 __global__ void k_extend_step(Job *J, DevParams P, char *arena, int64_t bytes, int r) {
   if (J->status != ST_OK || J->next_read != r) return;
-  const int32_t st = extend_one(J, P, arena, bytes, J->reads + J->read_off[r], J->read_len[r], r);
-  if (st != ST_OK && (threadIdx.x & 31) == 0) J->status = st;
+  int32_t st = extend_one(J, P, arena, bytes, J->reads + J->read_off[r], J->read_len[r], r, warp_smem());
+  if ((threadIdx.x & 31) == 0) {
+    if ((st == ST_OK && r + 1 == J->n_reads) || is_alignment_error(st)) {
+      const int32_t fs = finalize_order(J, arena, bytes);
+      if (st == ST_OK) st = fs;
+    }
+    if (st != ST_OK) J->status = st;
+  }
 }
 
 // extend_graph over reads r0..r1-1 held in a caller buffer.
 __global__ void k_extend_range(Job *J, DevParams P, char *arena, int64_t bytes, const uint8_t *reads,
                                const int64_t *read_off, const int32_t *read_len, int r0, int r1) {
+  int32_t st = ST_OK;
   for (int r = r0; r < r1; ++r) {
-    const int32_t st = extend_one(J, P, arena, bytes, reads + read_off[r], read_len[r], r);
-    if (st != ST_OK) {
-      if ((threadIdx.x & 31) == 0) J->status = st;
-      return;
+    st = extend_one(J, P, arena, bytes, reads + read_off[r], read_len[r], r, warp_smem());
+    if (st != ST_OK) break;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (st == ST_OK || is_alignment_error(st)) {
+      const int32_t fs = finalize_order(J, arena, bytes);
+      if (st == ST_OK) st = fs;
     }
+    if (st != ST_OK) J->status = st;
   }
 }
 
@@ -66,11 +92,13 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
   Work cells{};
   int32_t st;
   if (mode == 0) {
-    st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells);
+    st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, warp_smem());
   } else if (retry) {
-    st = poa_retry(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, s, &n_items, &cells);
+    st = poa_retry(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, s, &n_items, &cells,
+                   warp_smem());
   } else {
-    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, P.f, s, &n_items, &cells);
+    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, P.f, s, &n_items, &cells,
+                   warp_smem());
   }
   if (st == ST_OK)
     for (int k = lane; k < n_items; k += 32) out[k] = s.items[k];
@@ -84,7 +112,7 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
   }
 }
 
-__global__ void k_add_path(Job *J, DevParams P, int seq_id, const int4 *items, int n) {
+__global__ void k_add_path(Job *J, DevParams P, int seq_id, int4 *items, int n) {
   if (threadIdx.x == 0) J->status = add_path(J, P, seq_id, items, n);
 }
 
@@ -118,6 +146,7 @@ __global__ void k_toposort(Job *J, char *arena, int64_t bytes) {
     }
     int32_t *deg = reinterpret_cast<int32_t *>(arena);
     J->status = toposort(J, deg, deg + J->n_nodes);
+    J->order_exact = 1;
   }
 }
 
@@ -142,38 +171,46 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   J->n_items = 0;
   J->cells = 0;
   J->dp_bytes = 0;
+  J->order_exact = 1;
 }
 
 cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *queue, const DevParams &P,
                          char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
   const int blocks = (slots + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-  k_batch<<<blocks, WARPS_PER_BLOCK * 32, 0, stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, queue, P, arenas,
-                                                         slot_bytes);
+  const size_t smem = WARPS_PER_BLOCK * sizeof(WarpSmem);
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_batch<<<blocks, WARPS_PER_BLOCK * 32, smem, stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, queue, P,
+                                                          arenas, slot_bytes, slots);
   return cudaGetLastError();
 }
 
 cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,
                                cudaStream_t stream) {
-  k_extend_step<<<1, 32, 0, stream>>>(job_dev, P, arena, bytes, read);
+  k_extend_step<<<1, 32, sizeof(WarpSmem), stream>>>(job_dev, P, arena, bytes, read);
   return cudaGetLastError();
 }
 
 cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *reads,
                                 const int64_t *read_off, const int32_t *read_len, int r0, int r1,
                                 cudaStream_t stream) {
-  k_extend_range<<<1, 32, 0, stream>>>(job_dev, P, arena, bytes, reads, read_off, read_len, r0, r1);
+  k_extend_range<<<1, 32, sizeof(WarpSmem), stream>>>(job_dev, P, arena, bytes, reads, read_off, read_len, r0, r1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q, int qlen,
                          int mode, int beg_id, int end_id, int adaptive, uint64_t band_b, int retry, int4 *out,
                          int32_t *out_n, cudaStream_t stream) {
-  k_align<<<1, 32, 0, stream>>>(job_dev, P, arena, bytes, q, qlen, mode, beg_id, end_id, adaptive, band_b, retry,
-                                 out, out_n);
+  k_align<<<1, 32, sizeof(WarpSmem), stream>>>(job_dev, P, arena, bytes, q, qlen, mode, beg_id, end_id, adaptive,
+                                               band_b, retry, out, out_n);
   return cudaGetLastError();
 }
 
-cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, const int4 *items, int n,
+cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, int4 *items, int n,
                             cudaStream_t stream) {
   k_add_path<<<1, 32, 0, stream>>>(job_dev, P, seq_id, items, n);
   return cudaGetLastError();
