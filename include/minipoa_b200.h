@@ -158,6 +158,25 @@ int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *r
                      int64_t *in_cnt, int64_t *out_cnt, int64_t *in_pairs, int64_t *out_pairs, int64_t *path_seq,
                      int64_t *path_len, int64_t *path_ids);
 
+/* No counterpart in the reference. poa_align for callers that cannot
+ * allocate device memory when they align (a serving loop whose device memory
+ * belongs to another allocator, a strict memory budget, or a thread that must
+ * not trigger the device-wide synchronisation of cudaMalloc/cudaFree). The
+ * call allocates no device memory: its DP scratch and scoring tables sit in one
+ * library-owned array of POA_NOALLOC_SCRATCH_BYTES in device memory, which
+ * every GPU that loads the library keeps until the process exits. d_query
+ * (len bytes), d_out (out_cap >= len + 1 items) and d_out_len are device
+ * pointers owned by the caller; the graph must be toposorted, as for
+ * poa_align. The result equals poa_align's. A graph and query whose scratch
+ * would exceed the array are rejected with POA_ERR_ALLOC and a message (use
+ * poa_align then). The first call on a device looks up the array's device
+ * address; make that first call before any stream capture. Calls share the
+ * array: calls whose GPU work overlaps race and must be serialised by the
+ * caller. The context's device must be the current device. */
+#define POA_NOALLOC_SCRATCH_BYTES (32u << 20)
+int poa_align_noalloc(poa_ctx *ctx, const poa_params *params, poa_graph *graph, const uint8_t *d_query, int64_t len,
+                      poa_aligned_base *d_out, int64_t out_cap, int64_t *d_out_len);
+
 /* ---- batched independent read sets (no reference counterpart: the
  * reference runs one set per process; each set here is one extend_graph). */
 typedef struct poa_batch_stats {

@@ -1241,3 +1241,42 @@ int poa_batch_transfer_bytes(poa_ctx *ctx, poa_batch *b, uint64_t *h2d, uint64_t
 void poa_batch_free(poa_batch *batch) { delete batch; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Accessors for entry points defined in other translation units.
+namespace poa {
+
+Job *graph_device_job(poa_graph *g) { return g->d_job; }
+int graph_alphabet(const poa_graph *g) { return g->sigma; }
+cudaStream_t ctx_stream(const poa_ctx *c) { return c->stream; }
+int ctx_device(const poa_ctx *c) { return c->device; }
+void ctx_set_error(poa_ctx *c, const std::string &msg) { c->err = msg; }
+std::string describe_status(int32_t st, int err_i, int err_j) { return status_message(st, err_i, err_j); }
+int status_to_code(int32_t st) { return status_code(st); }
+
+// Copies the graph's device descriptor to *out (device-to-host copy, no
+// allocation); false with *err set on a CUDA failure.
+bool graph_read_job(poa_graph *g, Job *out, std::string *err) {
+  try {
+    g->sync();
+    *out = g->h;
+    return true;
+  } catch (const CudaError &e) {
+    *err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    return false;
+  }
+}
+
+// Clears a device-side error status left on the graph descriptor.
+bool graph_clear_status(poa_graph *g, std::string *err) {
+  try {
+    g->h.status = ST_OK;
+    g->upload();
+    return true;
+  } catch (const CudaError &e) {
+    *err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    return false;
+  }
+}
+
+}  // namespace poa

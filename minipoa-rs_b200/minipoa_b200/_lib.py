@@ -72,6 +72,7 @@ SIGNATURES = {
     "poa_batch_graph": (ctypes.c_int, [_vp, _vp, _i64, P(_vp)]),
     "poa_batch_free": (None, [_vp]),
     "poa_batch_tune": (ctypes.c_int, [_vp, _vp, _i32, _u64]),
+    "poa_align_noalloc": (ctypes.c_int, [_vp, _cp, _vp, _vp, _i64, _vp, _i64, _vp]),
     "poa_batch_transfer_bytes": (ctypes.c_int, [_vp, _vp, P(_u64), P(_u64)]),
 }
 
