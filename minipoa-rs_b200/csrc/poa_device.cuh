@@ -119,6 +119,7 @@ struct Scratch {
   int4 *pmeta;         // per pred entry: (row, band start, band length, -)
   int64_t *pmeta_off;  // per pred entry: the predecessor row's arena offset
   int32_t *seq;        // encoded, padded query
+  uint8_t *seq8;       // the same, one byte per column (when it does not fit shared memory)
   int4 *items;         // alignment result (node, base, aligned, resolved id)
   char *dp;            // DP matrix cells
   int64_t dp_bytes;
@@ -161,6 +162,7 @@ __device__ inline bool carve_scratch(char *arena, int64_t bytes, int n, int e, i
   s.pmeta = (int4 *)take(int64_t(e + 1) * 16);
   s.pmeta_off = (int64_t *)take(int64_t(e + 1) * 8);
   s.seq = (int32_t *)take((padded + 32) * 4);
+  s.seq8 = (uint8_t *)take(padded + 32);
   s.items = (int4 *)take((n_items + 1) * 16);
   s.dp = arena + o;
   s.dp_bytes = bytes - o;
@@ -283,6 +285,195 @@ __device__ inline int32_t add_path(Job *J, const DevParams &P, int seq_id, int4 
   return ST_OK;
 }
 
+// add_path (graph.rs:82-122) by the whole warp, one item per lane. It covers
+// the case every alignment path is in: the items name pairwise distinct
+// nodes. That holds when the pre-existing nodes of the path have strictly
+// increasing ranks, no item names the sink, and no two items create the same
+// column sibling (same parent and base); those three facts are checked first,
+// and when one fails nothing has been changed and false is returned, so the
+// caller runs the serial add_path. With distinct nodes every node gains at
+// most one incoming and one outgoing edge, so the edges are independent and
+// each lane appends its own; new node ids are handed out in path order by a
+// prefix count, as the serial loop does. Edge-list chunks may be numbered in
+// another order than the serial loop numbers them; chunk numbers are storage
+// only, the lists keep their insertion order. Invalid items and capacity
+// give the serial function's status (true is returned, graph unchanged).
+__device__ inline bool add_path_warp(Job *J, const DevParams &P, int seq_id, int4 *items, int n, int32_t *status) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int n_old = J->n_nodes;
+  *status = ST_OK;
+  for (int t0 = 0; t0 < n; t0 += 32) {
+    const int t = t0 + lane;
+    int code = ST_OK;
+    if (t < n) {
+      const int4 it = items[t];
+      if (it.y < 0 || it.y >= P.sigma)
+        code = ST_BASE_OUTSIDE;
+      else if ((it.x >= 0 && it.x >= n_old) || (it.z >= 0 && it.z >= n_old))
+        code = ST_UNKNOWN_NODE;
+    }
+    const unsigned bad = __ballot_sync(FULL, code != ST_OK);
+    if (bad) {
+      *status = __shfl_sync(FULL, code, __ffs(bad) - 1);
+      return true;
+    }
+  }
+  if (n_old + n > J->node_cap || J->n_chunks + 2 * (n + 1) > J->chunk_cap || J->path_used + n > J->path_cap ||
+      J->n_paths + 1 > J->max_paths) {
+    *status = ST_GRAPH_FULL;
+    return true;
+  }
+  // resolve: .w = node id (existing), -1 (new node), -(parent + 2) (new
+  // column sibling, whose (parent, base) slot of `aligned` is claimed)
+  bool ok = true;
+  int rank_carry = -1;
+  for (int t0 = 0; t0 < n; t0 += 32) {
+    const int t = t0 + lane;
+    int w = -1, rk = -1;
+    bool fail = false;
+    if (t < n) {
+      const int4 it = items[t];
+      if (it.x >= 0) {
+        w = it.x;
+      } else if (it.z >= 0) {
+        const int parent = J->parent[it.z];
+        int32_t *slot = &J->aligned[int64_t(parent) * P.sigma + it.y];
+        const int a = *slot;
+        if (a >= 0) {
+          w = a;
+        } else {
+          w = -(parent + 2);
+          fail = atomicMin(slot, INT32_MIN + t) != -1;  // another item claimed it first
+        }
+      }
+      if (w >= 0) {
+        rk = J->rank[w];
+        fail = fail || w == 1;
+      }
+      items[t].w = w;
+    }
+    int pm = rk;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(FULL, pm, d);
+      if (lane >= d) pm = max(pm, v);
+    }
+    int before = __shfl_up_sync(FULL, pm, 1);
+    if (lane == 0) before = -1;
+    before = max(before, rank_carry);
+    if (w >= 0 && rk <= before) fail = true;
+    rank_carry = max(rank_carry, __shfl_sync(FULL, pm, 31));
+    if (__any_sync(FULL, fail)) ok = false;
+  }
+  __syncwarp();
+  if (!ok) {
+    for (int t = lane; t < n; t += 32) {
+      const int4 it = items[t];
+      if (it.w <= -2) atomicExch(&J->aligned[int64_t(-(it.w + 2)) * P.sigma + it.y], -1);
+    }
+    __syncwarp();
+    return false;
+  }
+  // nodes, in path order
+  const int path_base = J->path_used;
+  int new_carry = 0, path_carry = 0;
+  for (int t0 = 0; t0 < n; t0 += 32) {
+    const int t = t0 + lane;
+    int4 it = make_int4(0, 0, 0, 0);
+    if (t < n) it = items[t];
+    const bool fresh = t < n && it.w < 0;
+    const unsigned fm = __ballot_sync(FULL, fresh);
+    int id = it.w;
+    if (fresh) {
+      id = n_old + new_carry + __popc(fm & lt);
+      const int parent = it.w <= -2 ? -(it.w + 2) : id;
+      J->base[id] = uint8_t(it.y);
+      J->parent[id] = parent;
+      J->rank[id] = 0;
+      J->coverage[id] = 0;
+      for (int c = 0; c < P.sigma; ++c) J->aligned[int64_t(id) * P.sigma + c] = c == it.y ? id : -1;
+      J->in_cnt[id] = 0;
+      J->out_cnt[id] = 0;
+      J->in_head[id] = J->in_tail[id] = -1;
+      J->out_head[id] = J->out_tail[id] = -1;
+      if (it.w <= -2) J->aligned[int64_t(parent) * P.sigma + it.y] = id;
+      items[t].w = id;
+    }
+    const bool on_path = t < n && id >= 2;
+    const unsigned pmask = __ballot_sync(FULL, on_path);
+    if (on_path) J->path_items[path_base + path_carry + __popc(pmask & lt)] = id;
+    new_carry += __popc(fm);
+    path_carry += __popc(pmask);
+  }
+  __syncwarp();
+  // edges k = 1..K: items[k-1] -> items[k], and the last item (or the
+  // source) -> sink
+  const int K = n > 0 ? n : 1;
+  int chunk_carry = J->n_chunks, in_added = 0;
+  for (int k0 = 1; k0 <= K; k0 += 32) {
+    const int k = k0 + lane;
+    const bool live = k <= K;
+    int from = 0, to = 1;
+    if (live) {
+      from = n > 0 ? items[k - 1].w : 0;
+      to = k < n ? items[k].w : 1;
+    }
+    const bool act = live && from != to;
+    bool out_new = false, in_new = false;
+    if (act) {
+      // a list of a pre-existing node cannot hold a new node yet
+      const bool both_old = from < n_old && to < n_old;
+      out_new = !(both_old && list_bump(J, J->out_head, J->out_cnt, from, to));
+      in_new = !(both_old && list_bump(J, J->in_head, J->in_cnt, to, from));
+    }
+    const int oc = out_new ? J->out_cnt[from] : 1, ic = in_new ? J->in_cnt[to] : 1;
+    const int need = int(out_new && oc % CHUNK == 0) + int(in_new && ic % CHUNK == 0);
+    int inc = need;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(FULL, inc, d);
+      if (lane >= d) inc += v;
+    }
+    int ch = chunk_carry + inc - need;
+    auto append = [&](int32_t *head, int32_t *tail, int32_t *cnt, int node, int id, int c) {
+      const int slot = c % CHUNK;
+      int chunk;
+      if (slot == 0) {
+        chunk = ch++;
+        J->chunk_next[chunk] = -1;
+        if (c == 0)
+          head[node] = chunk;
+        else
+          J->chunk_next[tail[node]] = chunk;
+        tail[node] = chunk;
+      } else {
+        chunk = tail[node];
+      }
+      J->chunk_id[int64_t(chunk) * CHUNK + slot] = id;
+      J->chunk_w[int64_t(chunk) * CHUNK + slot] = 1;
+      cnt[node] = c + 1;
+    };
+    if (out_new) append(J->out_head, J->out_tail, J->out_cnt, from, to, oc);
+    if (in_new) append(J->in_head, J->in_tail, J->in_cnt, to, from, ic);
+    if (act) J->coverage[to] += 1;
+    chunk_carry += __shfl_sync(FULL, inc, 31);
+    in_added += __popc(__ballot_sync(FULL, in_new));
+  }
+  __syncwarp();
+  if (lane == 0) {
+    J->n_nodes = n_old + new_carry;
+    J->path_used = path_base + path_carry;
+    J->n_chunks = chunk_carry;
+    J->n_edges += in_added;
+    J->path_seq[J->n_paths] = seq_id;
+    J->path_off[J->n_paths + 1] = J->path_used;
+    J->n_paths += 1;
+  }
+  __syncwarp();
+  return true;
+}
+
 // graph.rs:125-178 with grouped = false (lane 0); LIFO Kahn over
 // incoming-list degrees, successors pushed in outgoing order.
 __device__ inline int32_t toposort(Job *J, int32_t *deg, int32_t *stack) {
@@ -358,7 +549,7 @@ __device__ __forceinline__ T mins(T a, T b) {
 // update and the traceback skip them, as the reference's head filter does.
 // (head or tail, support) of the last GRING rows live in a shared-memory
 // ring so the serial passes read their neighbours without an L2 round trip.
-constexpr int GRING = 64;
+constexpr int GRING = 32;
 __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int n, int64_t *ring_v,
                                  int64_t *ring_s) {
   const int lane = threadIdx.x & 31;
@@ -368,17 +559,54 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
     int cin = 0, cout = 0;
     int64_t wsum = 0;
     int node = -1;
+    // the first chunk of each list (CHUNK entries) is read as vectors; longer
+    // lists are walked again below
+    int4 in_id = make_int4(0, 0, 0, 0), in_w = in_id, out_id = in_id, out_w = in_id;
+    int in_n = 0, out_n = 0, in_r[CHUNK] = {0, 0, 0, 0}, out_r[CHUNK] = {0, 0, 0, 0};
     if (i < n) {
       node = J->rank_to_node[beg + i];
-      for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
-        wsum += w;
-        const int r = J->rank[pred];
-        if (r >= beg && r < beg + i) ++cin;
-      });
-      for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int) {
-        const int r = J->rank[succ];
-        if (r > beg + i && r <= end) ++cout;
-      });
+      in_n = J->in_cnt[node];
+      out_n = J->out_cnt[node];
+      const int ih = J->in_head[node], oh = J->out_head[node];
+      if (in_n > 0) {
+        in_id = *reinterpret_cast<const int4 *>(J->chunk_id + int64_t(ih) * CHUNK);
+        in_w = *reinterpret_cast<const int4 *>(J->chunk_w + int64_t(ih) * CHUNK);
+      }
+      if (out_n > 0) {
+        out_id = *reinterpret_cast<const int4 *>(J->chunk_id + int64_t(oh) * CHUNK);
+        out_w = *reinterpret_cast<const int4 *>(J->chunk_w + int64_t(oh) * CHUNK);
+      }
+      const int iid[CHUNK] = {in_id.x, in_id.y, in_id.z, in_id.w};
+      const int iw[CHUNK] = {in_w.x, in_w.y, in_w.z, in_w.w};
+      const int oid[CHUNK] = {out_id.x, out_id.y, out_id.z, out_id.w};
+#pragma unroll
+      for (int k = 0; k < CHUNK; ++k) {
+        if (k < in_n) in_r[k] = J->rank[iid[k]];
+        if (k < out_n) out_r[k] = J->rank[oid[k]];
+      }
+#pragma unroll
+      for (int k = 0; k < CHUNK; ++k) {
+        if (k < in_n) {
+          wsum += iw[k];
+          if (in_r[k] >= beg && in_r[k] < beg + i) ++cin;
+        }
+        if (k < out_n && out_r[k] > beg + i && out_r[k] <= end) ++cout;
+      }
+      if (in_n > CHUNK || out_n > CHUNK) {
+        int k = 0;
+        for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
+          if (k++ < CHUNK) return;
+          wsum += w;
+          const int r = J->rank[pred];
+          if (r >= beg && r < beg + i) ++cin;
+        });
+        k = 0;
+        for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int) {
+          if (k++ < CHUNK) return;
+          const int r = J->rank[succ];
+          if (r > beg + i && r <= end) ++cout;
+        });
+      }
     }
     int pin = cin, pout = cout;
 #pragma unroll
@@ -397,16 +625,28 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
       s.succ_start[i] = ss;
       s.succ_cnt[i] = cout;
       s.wsum[i] = wsum;
-      int k = ps;
-      for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
-        const int r = J->rank[pred];
-        if (r >= beg && r < beg + i) s.pred[k++] = make_int2(r - beg, w);
-      });
-      k = ss;
-      for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int w) {
-        const int r = J->rank[succ];
-        if (r > beg + i && r <= end) s.succ[k++] = make_int2(r - beg, w);
-      });
+      int kp = ps, ks = ss;
+      const int iw[CHUNK] = {in_w.x, in_w.y, in_w.z, in_w.w};
+      const int ow[CHUNK] = {out_w.x, out_w.y, out_w.z, out_w.w};
+#pragma unroll
+      for (int k = 0; k < CHUNK; ++k) {
+        if (k < in_n && in_r[k] >= beg && in_r[k] < beg + i) s.pred[kp++] = make_int2(in_r[k] - beg, iw[k]);
+        if (k < out_n && out_r[k] > beg + i && out_r[k] <= end) s.succ[ks++] = make_int2(out_r[k] - beg, ow[k]);
+      }
+      if (in_n > CHUNK || out_n > CHUNK) {
+        int k = 0;
+        for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int w) {
+          if (k++ < CHUNK) return;
+          const int r = J->rank[pred];
+          if (r >= beg && r < beg + i) s.pred[kp++] = make_int2(r - beg, w);
+        });
+        k = 0;
+        for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int w) {
+          if (k++ < CHUNK) return;
+          const int r = J->rank[succ];
+          if (r > beg + i && r <= end) s.succ[ks++] = make_int2(r - beg, w);
+        });
+      }
       s.head[i] = NEG64;
       s.tail[i] = NEG64;
       s.support[i] = 0;
@@ -415,28 +655,53 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
     sbase += __shfl_sync(FULL, pout, 31);
   }
   __syncwarp();
-  int32_t st = ST_OK;
-  if (lane == 0) {
-    int64_t *rv = ring_v, *rs = ring_s;
-    s.head[0] = 0;
-    if (rv) {
-      rv[0] = 0;
-      rs[0] = 0;
+  // The serial passes run on every lane in lockstep (each lane computes the
+  // same values and writes the same words, so it only ever reads its own
+  // writes). Lane l holds the list start, count and first two entries of row
+  // i0 + l of the current 32-row block, loaded one block ahead, and the rows
+  // read them by shuffle; (head or tail, support) of the last GRING rows sit
+  // in the shared-memory ring.
+  int64_t *rv = ring_v, *rsu = ring_s;
+  struct Lists {
+    int start, cnt;
+    int2 e0, e1;
+  };
+  auto load = [&](const int32_t *st, const int32_t *ct, const int2 *ent, int r, bool ok) {
+    Lists L{0, 0, make_int2(-1, 0), make_int2(-1, 0)};
+    if (ok) {
+      L.start = st[r];
+      L.cnt = ct[r];
+      if (L.cnt > 0) L.e0 = ent[L.start];
+      if (L.cnt > 1) L.e1 = ent[L.start + 1];
     }
-    for (int i = 1; i < n; ++i) {
+    return L;
+  };
+  // forward: head along the heaviest (then most supported) predecessor
+  s.head[0] = 0;
+  rv[0] = 0;
+  rsu[0] = 0;
+  Lists nxt = load(s.pred_start, s.pred_cnt, s.pred, 1 + lane, 1 + lane < n);
+  for (int i0 = 1; i0 < n; i0 += 32) {
+    const Lists cur = nxt;
+    nxt = load(s.pred_start, s.pred_cnt, s.pred, i0 + 32 + lane, i0 + 32 + lane < n);
+    const int lim = min(32, n - i0);
+    for (int k = 0; k < lim; ++k) {
+      const int i = i0 + k;
+      const int pb = __shfl_sync(FULL, cur.start, k), pc = __shfl_sync(FULL, cur.cnt, k);
+      const int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, k), __shfl_sync(FULL, cur.e0.y, k));
+      const int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, k), __shfl_sync(FULL, cur.e1.y, k));
       bool have = false;
       int bw = 0;
       int64_t bsup = 0, bhead = 0;
-      const int pb = s.pred_start[i], pc = s.pred_cnt[i];
       for (int t = 0; t < pc; ++t) {
-        const int2 e = s.pred[pb + t];
-        const bool near = rv && i - e.x < GRING;
+        const int2 e = t == 0 ? f0 : (t == 1 ? f1 : s.pred[pb + t]);
+        const bool near = i - e.x < GRING;
         const int64_t hp = near ? rv[e.x & (GRING - 1)] : s.head[e.x];
         if (hp == NEG64) {
           s.pred[pb + t].x = -1;
           continue;
         }
-        const int64_t sp = near ? rs[e.x & (GRING - 1)] : s.support[e.x];
+        const int64_t sp = near ? rsu[e.x & (GRING - 1)] : s.support[e.x];
         if (!have || e.y > bw || (e.y == bw && sp > bsup)) {
           have = true;
           bw = e.y;
@@ -450,24 +715,33 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
         s.head[i] = hi;
         s.support[i] = si;
       }
-      if (rv) {
-        rv[i & (GRING - 1)] = hi;
-        rs[i & (GRING - 1)] = si;
-      }
+      rv[i & (GRING - 1)] = hi;
+      rsu[i & (GRING - 1)] = si;
     }
-    s.tail[n - 1] = 1;
-    if (rv) rv[(n - 1) & (GRING - 1)] = 1;  // rs keeps the forward support of the last row
-    for (int i = n - 2; i >= 0; --i) {
+  }
+  // backward: tail along the heaviest (then most supported) successor; the
+  // support array continues from the forward pass
+  s.tail[n - 1] = 1;
+  rv[(n - 1) & (GRING - 1)] = 1;  // rsu keeps the forward support of the last row
+  nxt = load(s.succ_start, s.succ_cnt, s.succ, n - 2 - lane, n - 2 - lane >= 0);
+  for (int i0 = n - 2; i0 >= 0; i0 -= 32) {
+    const Lists cur = nxt;
+    nxt = load(s.succ_start, s.succ_cnt, s.succ, i0 - 32 - lane, i0 - 32 - lane >= 0);
+    const int lim = min(32, i0 + 1);
+    for (int k = 0; k < lim; ++k) {
+      const int i = i0 - k;
+      const int sb = __shfl_sync(FULL, cur.start, k), sn = __shfl_sync(FULL, cur.cnt, k);
+      const int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, k), __shfl_sync(FULL, cur.e0.y, k));
+      const int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, k), __shfl_sync(FULL, cur.e1.y, k));
       bool have = false;
       int bw = 0;
       int64_t bsup = 0, btail = 0;
-      const int sb = s.succ_start[i], sn = s.succ_cnt[i];
       for (int t = 0; t < sn; ++t) {
-        const int2 e = s.succ[sb + t];
-        const bool near = rv && e.x - i < GRING;
+        const int2 e = t == 0 ? f0 : (t == 1 ? f1 : s.succ[sb + t]);
+        const bool near = e.x - i < GRING;
         const int64_t ts = near ? rv[e.x & (GRING - 1)] : s.tail[e.x];
         if (ts == NEG64) continue;
-        const int64_t ss = near ? rs[e.x & (GRING - 1)] : s.support[e.x];
+        const int64_t ss = near ? rsu[e.x & (GRING - 1)] : s.support[e.x];
         if (!have || e.y > bw || (e.y == bw && ss > bsup)) {
           have = true;
           bw = e.y;
@@ -481,16 +755,12 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
         s.tail[i] = ti;
         s.support[i] = si;
       }
-      if (rv) {
-        rv[i & (GRING - 1)] = ti;
-        rs[i & (GRING - 1)] = si;
-      }
+      rv[i & (GRING - 1)] = ti;
+      rsu[i & (GRING - 1)] = si;
     }
-    if (s.head[n - 1] == NEG64) st = ST_NO_PATH;
   }
-  st = __shfl_sync(FULL, st, 0);
   __syncwarp();
-  return st;
+  return s.head[n - 1] == NEG64 ? ST_NO_PATH : ST_OK;
 }
 
 // align.rs:829-897 (lane 0): band state after row i peaked at `maximum`.
@@ -532,135 +802,208 @@ __device__ inline void adaptive_update(const Job *J, Scratch &s, int beg, int i,
   }
 }
 
-// Traceback of align.rs:1164-1347 (lane 0), reading the stored DP states.
-// Writes the path (source first, sink entry dropped) to s.items.
+// Traceback of align.rs:1164-1347 by the whole warp, reading the stored DP
+// states. Each step is the reference's decision sequence (preferred match,
+// deletion open / extend, insertion open / extend, match); lane t examines
+// predecessor t of the current row in parallel, and the reference's choose()
+// -- the first predecessor of largest weight among those whose state explains
+// the cell -- becomes a ballot plus a max-reduction over the lanes. While the
+// predecessors' states are loaded, each lane also loads the row descriptor
+// its predecessor would need as the next row, so a step costs two dependent
+// memory round trips. Steps are recorded as (row, column, kind) and resolved
+// into AlignedBase items (push_diagonal, align.rs:1316-1347) by a parallel
+// pass at the end, which also reverses them and prepends the source.
 template <typename S>
 __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A, int beg, int n, int64_t m,
-                             int *n_out) {
+                             const int32_t *mat, int *n_out) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
+  const int lane = threadIdx.x & 31;
   const int64_t neg_half = int64_t(NEGV) / 2;
-  auto contains = [&](int r, int64_t c) -> bool {
-    const int st = s.row_start[r];
-    return c >= st && c - st < s.row_len[r];
-  };
-  auto Mv = [&](int r, int64_t c) -> int64_t {
-    return contains(r, c) ? int64_t(A[s.row_off[r] + (c - s.row_start[r])]) : int64_t(NEGV);
-  };
-  auto Dv = [&](int r, int64_t c) -> int64_t {
-    return contains(r, c) ? int64_t(A[s.row_off[r] + s.row_len[r] + (c - s.row_start[r])]) : int64_t(NEGV);
-  };
-  auto Iv = [&](int r, int64_t c) -> int64_t {
-    return contains(r, c) ? int64_t(A[s.row_off[r] + 2 * int64_t(s.row_len[r]) + (c - s.row_start[r])])
-                          : int64_t(NEGV);
-  };
   const int64_t O = P.gap_open, E = P.gap_ext;
+  constexpr int KIND_INS = 0, KIND_DIAG = 1;
   int i = n - 1;
-  int64_t j = m - 1;
+  int j = int(m - 1);
   int op = OP_ALL;
   int nres = 0;
   int64_t steps = 0;
   int4 *res = s.items;
+  // descriptor of the current row
+  int rs = s.row_start[i], rl = s.row_len[i], pb = s.pred_start[i], pc = s.pred_cnt[i], rb = s.row_base[i];
+  int64_t ro = s.row_off[i], ws = s.wsum[i];
+  auto at = [&](int64_t off, int start, int len, int plane, int c) -> int64_t {
+    return (c >= start && c - start < len) ? int64_t(A[off + int64_t(plane) * len + (c - start)]) : int64_t(NEGV);
+  };
+  int32_t st = ST_OK;
   while (i > 0 || j > 0) {
     steps += 1;
-    if (steps > int64_t(n) + m) return ST_TB_NO_ADVANCE;
-    if (!contains(i, j) || Mv(i, j) <= neg_half) return ST_TB_LEFT_BAND;
-    const int node = J->rank_to_node[beg + i];
-    const int nb = J->base[node];
-    const int base = (i == n - 1) ? P.unknown : nb;
+    if (steps > int64_t(n) + m) {
+      st = ST_TB_NO_ADVANCE;
+      break;
+    }
+    const bool in_ij = j >= rs && j - rs < rl;
+    if (!in_ij) {
+      st = ST_TB_LEFT_BAND;
+      break;
+    }
+    const int64_t Mij = at(ro, rs, rl, 0, j), Dij = at(ro, rs, rl, 1, j), Iij = at(ro, rs, rl, 2, j);
+    if (Mij <= neg_half) {
+      st = ST_TB_LEFT_BAND;
+      break;
+    }
     const int qb = s.seq[j];
-    const int64_t score = P.matrix[base * P.sigma + qb];
-    const int pb = s.pred_start[i], pc = s.pred_cnt[i];
-    // choose(): first max-weight predecessor whose stored state explains
-    // (state, penalty) at column pj (align.rs:1201-1225).
-    auto choose = [&](int state, int64_t penalty, int64_t pj, int &bp_out, int &bw_out) -> bool {
-      bool found = false;
-      int bp = -1, bw = 0;
-      const int64_t target = state == OP_MATCH ? Mv(i, j) : Dv(i, j);
-      for (int t = 0; t < pc; ++t) {
-        const int2 e = s.pred[pb + t];
-        if (e.x < 0 || !contains(e.x, pj)) continue;
-        const int64_t source = state == OP_DELETE ? Dv(e.x, pj) : Mv(e.x, pj);
-        if (target == source + penalty && (!found || e.y > bw)) {
-          found = true;
-          bp = e.x;
-          bw = e.y;
+    const int64_t score = mat[rb * P.sigma + qb];
+    // per-predecessor flags, chunks of 32 predecessors (one in almost all rows)
+    int m_lane = -1, m_w = 0, o_lane = -1, o_w = 0, x_lane = -1, x_w = 0;  // best lane + weight per kind
+    int m_chunk = 0, o_chunk = 0, x_chunk = 0;
+    int4 pm = make_int4(-1, 0, 0, 0);
+    int64_t poff = 0;
+    int4 pnext = make_int4(0, 0, 0, 0);  // (pred_start, pred_cnt, row_base, -) of the lane's predecessor
+    int64_t pws = 0;
+    for (int t0 = 0; t0 < pc; t0 += 32) {
+      const int t = t0 + lane;
+      int4 q = make_int4(-1, 0, 0, 0);
+      int64_t qoff = 0;
+      if (t < pc) {
+        q = s.pmeta[pb + t];
+        qoff = s.pmeta_off[pb + t];
+      }
+      bool fm = false, fo = false, fx = false;
+      if (q.x >= 0 && t0 == 0) {
+        pnext = make_int4(s.pred_start[q.x], s.pred_cnt[q.x], s.row_base[q.x], 0);
+        pws = s.wsum[q.x];
+      }
+      if (q.x >= 0) {
+        const int64_t Mpm = at(qoff, q.y, q.z, 0, j - 1);
+        const int64_t Mpj = at(qoff, q.y, q.z, 0, j), Dpj = at(qoff, q.y, q.z, 1, j);
+        const bool c1 = j - 1 >= q.y && j - 1 - q.y < q.z, c0 = j >= q.y && j - q.y < q.z;
+        fm = j > 0 && c1 && Mij == Mpm + score;
+        fo = c0 && Dij == Mpj + O;
+        fx = c0 && Dij == Dpj + E;
+      }
+      auto best = [&](bool f, int &bl, int &bw, int &bc) {
+        const unsigned msk = __ballot_sync(FULL, f);
+        if (!msk) return;
+        const int mx = __reduce_max_sync(FULL, f ? unsigned(q.w) : 0u);
+        const int l = __ffs(__ballot_sync(FULL, f && q.w == mx)) - 1;
+        if (bl < 0 || mx > bw) {
+          bl = l;
+          bw = mx;
+          bc = t0;
+        }
+      };
+      best(fm, m_lane, m_w, m_chunk);
+      best(fo, o_lane, o_w, o_chunk);
+      best(fx, x_lane, x_w, x_chunk);
+      if (t0 == 0) {
+        pm = q;
+        poff = qoff;
+      }
+    }
+    // moves to predecessor (lane l of chunk c); the next row's descriptor
+    auto move_to = [&](int l, int c) {
+      int4 q = pm;
+      int64_t qoff = poff;
+      if (c != 0) {
+        const int t = c + lane;
+        if (t < pc) {
+          q = s.pmeta[pb + t];
+          qoff = s.pmeta_off[pb + t];
         }
       }
-      bp_out = bp;
-      bw_out = bw;
-      return found;
-    };
-    auto push_diagonal = [&]() {
-      if (i == n - 1 && j != m - 1) {
-        res[nres++] = make_int4(-1, qb, -1, 0);
-      } else if (base == qb) {
-        res[nres++] = make_int4(node, nb, -1, 0);
+      i = __shfl_sync(FULL, q.x, l);
+      rs = __shfl_sync(FULL, q.y, l);
+      rl = __shfl_sync(FULL, q.z, l);
+      ro = __shfl_sync(FULL, (long long)qoff, l);
+      if (c == 0) {
+        pb = __shfl_sync(FULL, pnext.x, l);
+        pc = __shfl_sync(FULL, pnext.y, l);
+        rb = __shfl_sync(FULL, pnext.z, l);
+        ws = __shfl_sync(FULL, (long long)pws, l);
       } else {
-        const int parent = J->parent[node];
-        res[nres++] = make_int4(J->aligned[int64_t(parent) * P.sigma + qb], qb, parent, 0);
+        pb = s.pred_start[i];
+        pc = s.pred_cnt[i];
+        rb = s.row_base[i];
+        ws = s.wsum[i];
       }
     };
-    int kp, kw;
-    bool preferred = false;
-    if ((op & OP_MATCH) && j > 0 && base == qb) preferred = choose(OP_MATCH, score, j - 1, kp, kw);
-    if (preferred && !(int64_t(kw) >= s.wsum[i] / 10)) preferred = false;
-    if (preferred) {
-      push_diagonal();
-      i = kp;
+    if ((op & OP_MATCH) && j > 0 && rb == qb && m_lane >= 0 && int64_t(m_w) >= ws / 10) {
+      if (lane == 0) res[nres] = make_int4(i, j, KIND_DIAG, 0);
+      ++nres;
+      move_to(m_lane, m_chunk);
       j -= 1;
       op = OP_ALL;
       continue;
     }
-    if ((op & OP_DELETE) && (op == OP_DELETE || Mv(i, j) == Dv(i, j))) {
-      if (choose(OP_INSERT, O, j, kp, kw)) {
-        i = kp;
+    if ((op & OP_DELETE) && (op == OP_DELETE || Mij == Dij)) {
+      if (o_lane >= 0) {
+        move_to(o_lane, o_chunk);
         op = P.gap_open_raw == 0 ? OP_ALL : (OP_MATCH | OP_INSERT);
         continue;
       }
-      if (choose(OP_DELETE, E, j, kp, kw)) {
-        i = kp;
+      if (x_lane >= 0) {
+        move_to(x_lane, x_chunk);
         op = OP_DELETE;
         continue;
       }
     }
-    if ((op & OP_INSERT) && j > 0 && contains(i, j - 1) && (op == OP_INSERT || Mv(i, j) == Iv(i, j))) {
-      if (Iv(i, j) == Mv(i, j - 1) + O) {
-        res[nres++] = make_int4(-1, qb, -1, 0);
+    if ((op & OP_INSERT) && j > 0 && j - 1 >= rs && (op == OP_INSERT || Mij == Iij)) {
+      const int64_t Mim = at(ro, rs, rl, 0, j - 1), Iim = at(ro, rs, rl, 2, j - 1);
+      if (Iij == Mim + O) {
+        if (lane == 0) res[nres] = make_int4(i, j, KIND_INS, 0);
+        ++nres;
         j -= 1;
         op = P.gap_open_raw == 0 ? OP_ALL : (OP_MATCH | OP_DELETE);
         continue;
       }
-      if (Iv(i, j) == Iv(i, j - 1) + E) {
-        res[nres++] = make_int4(-1, qb, -1, 0);
+      if (Iij == Iim + E) {
+        if (lane == 0) res[nres] = make_int4(i, j, KIND_INS, 0);
+        ++nres;
         j -= 1;
         op = OP_INSERT;
         continue;
       }
     }
-    if ((op & OP_MATCH) && j > 0) {
-      if (choose(OP_MATCH, score, j - 1, kp, kw)) {
-        push_diagonal();
-        i = kp;
-        j -= 1;
-        op = OP_ALL;
-        continue;
-      }
+    if ((op & OP_MATCH) && j > 0 && m_lane >= 0) {
+      if (lane == 0) res[nres] = make_int4(i, j, KIND_DIAG, 0);
+      ++nres;
+      move_to(m_lane, m_chunk);
+      j -= 1;
+      op = OP_ALL;
+      continue;
     }
-    J->err_i = i;
-    J->err_j = int32_t(j);
-    return ST_TB_NO_PRED;
+    if (lane == 0) {
+      J->err_i = i;
+      J->err_j = j;
+    }
+    st = ST_TB_NO_PRED;
+    break;
   }
-  // result = reverse(pushed + [source]) without its last element.
-  for (int a = 0, b = nres - 1; a < b; ++a, --b) {
-    const int4 t = res[a];
-    res[a] = res[b];
-    res[b] = t;
+  __syncwarp();
+  if (st != ST_OK) return st;
+  // resolve, reverse, drop the sink entry (pushed first) and prepend the
+  // source: final[k] = resolve(pushed[nres - k]) for k = 1..nres-1
+  auto resolve = [&](int4 r) -> int4 {
+    const int qb = s.seq[r.y];
+    if (r.z == KIND_INS || (r.x == n - 1 && r.y != m - 1)) return make_int4(-1, qb, -1, 0);
+    const int node = J->rank_to_node[beg + r.x];
+    const int nb = J->base[node];
+    const int base = r.x == n - 1 ? P.unknown : nb;
+    if (base == qb) return make_int4(node, nb, -1, 0);
+    const int parent = J->parent[node];
+    return make_int4(J->aligned[int64_t(parent) * P.sigma + qb], qb, parent, 0);
+  };
+  for (int q = 1 + lane; 2 * q <= nres; q += 32) {
+    const int k = nres - q;
+    const int4 a = res[q], b = res[k];
+    res[k] = resolve(a);
+    if (k != q) res[q] = resolve(b);
   }
-  for (int k = nres - 1; k >= 1; --k) res[k] = res[k - 1];
-  if (nres > 0) {
+  __syncwarp();
+  if (nres > 0 && lane == 0) {
     const int src = J->rank_to_node[beg];
     res[0] = make_int4(src, J->base[src], -1, 0);
   }
+  __syncwarp();
   *n_out = nres;
   return ST_OK;
 }
@@ -676,145 +1019,194 @@ __device__ inline bool i32_scores_safe(const Job *J, const DevParams &P, int beg
   return steps <= SCORE_LIMIT / P.largest;
 }
 
-// Per-warp shared memory: the M and D states of the last RING_ROWS rows,
-// indexed by absolute query column modulo RING_W, so predecessor rows are
-// read from shared memory instead of L2/HBM (a slot is valid for row r only
-// while ring_row[r % RING_ROWS] == r); the scoring matrix; the guide rings.
-constexpr int RING_ROWS = 4;
-constexpr int RING_W = 512;
-constexpr int SMEM_MATRIX = 512;  // sigma^2 entries kept in shared memory (sigma <= 22)
+// Per-warp shared memory. The M and D states of the most recent rows live in
+// a ring of RING_CAP entries per state: rows are packed back to back in row
+// order, row r starting at entry (cumulative band length of rows < r) mod
+// RING_CAP, so a predecessor's states are read from shared memory instead of
+// L2/HBM while fewer than RING_CAP entries were written after it (about five
+// rows of the widest bands kept here, ten of 256 columns). Also the scoring
+// matrix, the guide-pass rings and the encoded query (one byte per column).
+constexpr int RING_CAP = 2560;
+constexpr int RING_MAX_LEN = 512;  // widest band computed by the striped row
+constexpr int SMEM_MATRIX = 512;   // sigma^2 entries kept in shared memory (sigma <= 22)
+constexpr int SEQ_SMEM = 5632;     // padded query columns kept in shared memory
 struct WarpSmem {
-  int32_t ring_m[RING_ROWS][RING_W];
-  int32_t ring_d[RING_ROWS][RING_W];
-  int32_t ring_row[RING_ROWS];
+  int32_t ring_m[RING_CAP];
+  int32_t ring_d[RING_CAP];
   int32_t matrix[SMEM_MATRIX];
   int64_t gring_v[GRING];  // guide passes: head (forward) or tail (backward)
   int64_t gring_s[GRING];  // guide passes: support
+  uint8_t seq8[SEQ_SMEM];
 };
 
-// One int32 DP row of at most 32*C columns (align.rs:751-828) as a blocked
-// register tile: lane l owns columns [start + C*l, start + C*l + C). The
-// predecessors (band, arena row and ring slot held by the lanes of `vmask`)
-// are folded into M and D; each lane scans its block serially, one warp
-// max-plus scan over the lane aggregates (shift C*E per lane) gives every
-// lane its carried-in insertion state, and a per-lane fixup finishes I and
-// M. All identities are exact in integers: I[j+1] = max(I[j] + E, md[j] + O)
+// Ring entry of column j of a row whose band starts at `start` and whose
+// first column sits at ring entry `pos`.
+__device__ __forceinline__ int ring_at(int pos, int start, int j) {
+  const int x = pos + (j - start);
+  return x >= RING_CAP ? x - RING_CAP : x;
+}
+
+// One int32 DP row of at most 128*G columns (align.rs:751-828) in stripes:
+// stripe g covers columns [start + 128g, start + 128g + 128) and lane l owns
+// the 4 consecutive columns at 4l of each stripe, so every shared-memory and
+// global access of a stripe is one contiguous 512-byte vector access. Bands
+// start and end on multiples of 8, so a lane's 4 columns lie wholly inside or
+// wholly outside any band. Predecessors (band, ring entry or arena row, held
+// by the lanes of `vmask`) are folded into M and D; each lane scans its 4
+// columns, a warp max-plus scan (shift 4E per lane) carries the insertion
+// state across the lanes of a stripe, and the stripes chain their carries.
+// All identities are exact in integers: I[j+1] = max(I[j] + E, md[j] + O)
 // with I[start] = NEG32.
-template <int C>
-__device__ __forceinline__ void dp_row_blocked(int lane, int start, int len, int32_t *R, const int32_t *seq,
+template <int G>
+__device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                                const int32_t *mrow, int32_t E, int32_t O, unsigned vmask,
-                                               int my_ps, int my_pl, int my_slot, const int32_t *my_g,
-                                               WarpSmem *sm, int out_slot, bool adapt, int32_t &bestv,
-                                               int &bestj) {
+                                               int my_ps, int my_pl, int my_pos, const int32_t *my_g,
+                                               WarpSmem *sm, int pos_i, bool adapt, int32_t &bestv, int &bestj) {
   const int stop = start + len;
-  const int j0 = start + C * lane;
-  int32_t Mx[C], Dx[C];
+  int32_t Mx[G][4], Dx[G][4];
 #pragma unroll
-  for (int k = 0; k < C; ++k) {
-    Mx[k] = NEG32;
-    Dx[k] = NEG32;
-  }
+  for (int g = 0; g < G; ++g)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      Mx[g][k] = NEG32;
+      Dx[g][k] = NEG32;
+    }
   while (vmask) {
     const int t = __ffs(vmask) - 1;
     vmask &= vmask - 1;
     const int ps = __shfl_sync(FULL, my_ps, t);
     const int pl = __shfl_sync(FULL, my_pl, t);
-    const int slot = __shfl_sync(FULL, my_slot, t);
-    const int32_t *g = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
-    if (slot >= 0) {
-      const int32_t *rm = sm->ring_m[slot];
-      const int32_t *rd = sm->ring_d[slot];
-      int32_t prev = (j0 > ps && j0 - 1 < ps + pl) ? rm[(j0 - 1) & (RING_W - 1)] : NEG32;
+    const int pos = __shfl_sync(FULL, my_pos, t);
+    const int32_t *gp = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
 #pragma unroll
-      for (int k = 0; k < C; ++k) {
-        const int j = j0 + k;
-        const bool in = unsigned(j - ps) < unsigned(pl);
-        const int32_t mp = rm[j & (RING_W - 1)], dp = rd[j & (RING_W - 1)];
-        if (in) {
-          Mx[k] = maxs(Mx[k], prev);
-          Dx[k] = maxs(Dx[k], maxs(dp + E, mp + O));
+    for (int g = 0; g < G; ++g) {
+      const int j0 = start + 128 * g + 4 * lane;
+      if (j0 < stop && j0 >= ps && j0 < ps + pl) {
+        int4 m4, d4;
+        int32_t prev = NEG32;
+        if (pos >= 0) {
+          const int x = ring_at(pos, ps, j0);
+          m4 = *reinterpret_cast<const int4 *>(sm->ring_m + x);
+          d4 = *reinterpret_cast<const int4 *>(sm->ring_d + x);
+          if (j0 > ps) prev = sm->ring_m[x == 0 ? RING_CAP - 1 : x - 1];
+        } else {
+          m4 = *reinterpret_cast<const int4 *>(gp + (j0 - ps));
+          d4 = *reinterpret_cast<const int4 *>(gp + pl + (j0 - ps));
+          if (j0 > ps) prev = gp[j0 - ps - 1];
         }
-        prev = in ? mp : NEG32;
-      }
-    } else {
-      int32_t prev = (j0 > ps && j0 - 1 < ps + pl) ? g[j0 - 1 - ps] : NEG32;
-#pragma unroll
-      for (int k = 0; k < C; ++k) {
-        const int j = j0 + k;
-        const bool in = unsigned(j - ps) < unsigned(pl);
-        int32_t mp = NEG32, dp = NEG32;
-        if (in) {
-          mp = g[j - ps];
-          dp = g[pl + j - ps];
-          Mx[k] = maxs(Mx[k], prev);
-          Dx[k] = maxs(Dx[k], maxs(dp + E, mp + O));
-        }
-        prev = mp;
+        Mx[g][0] = maxs(Mx[g][0], prev);
+        Mx[g][1] = maxs(Mx[g][1], m4.x);
+        Mx[g][2] = maxs(Mx[g][2], m4.y);
+        Mx[g][3] = maxs(Mx[g][3], m4.z);
+        Dx[g][0] = maxs(Dx[g][0], maxs(d4.x + E, m4.x + O));
+        Dx[g][1] = maxs(Dx[g][1], maxs(d4.y + E, m4.y + O));
+        Dx[g][2] = maxs(Dx[g][2], maxs(d4.z + E, m4.z + O));
+        Dx[g][3] = maxs(Dx[g][3], maxs(d4.w + E, m4.w + O));
       }
     }
   }
-  // md and the in-block scan x[k] = max over k' <= k of md[k'] + O + (k-k')E
-  int32_t X[C];
+  // md, the in-lane scan x[k] = max over k' <= k of md[k'] + O + (k-k')E, and
+  // per stripe the warp scan of the lane aggregates: pre[g] = the insertion
+  // state entering the lane's first column from the lanes before it (without
+  // the stripe's own carry; a value below every reachable state for lane 0)
+  constexpr int32_t BELOW = INT32_MIN / 2;
+  int32_t X[G][4], pre[G];
 #pragma unroll
-  for (int k = 0; k < C; ++k) {
-    const int j = j0 + k;
-    const int32_t prof = j < stop ? mrow[seq[j]] : 0;
-    Mx[k] = maxs(Mx[k] + prof, Dx[k]);  // Mx now holds md
-    X[k] = Mx[k] + O;
-    if (k > 0) X[k] = maxs(X[k], X[k - 1] + E);
-  }
-  // lane aggregates: y_l = max over k < start + C(l+1) of md[k] + O + shift
-  int32_t y = X[C - 1];
+  for (int g = 0; g < G; ++g) {
+    const int j0 = start + 128 * g + 4 * lane;
+    uint32_t bw = 0;
+    if (j0 < stop) bw = *reinterpret_cast<const uint32_t *>(seq8 + j0);
 #pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int32_t v = __shfl_up_sync(FULL, y, d);
-    if (lane >= d) y = maxs(y, v + d * C * E);
+    for (int k = 0; k < 4; ++k) {
+      const int32_t prof = j0 < stop ? mrow[(bw >> (8 * k)) & 0xff] : 0;
+      Mx[g][k] = maxs(Mx[g][k] + prof, Dx[g][k]);  // Mx now holds md
+      X[g][k] = Mx[g][k] + O;
+      if (k > 0) X[g][k] = maxs(X[g][k], X[g][k - 1] + E);
+    }
+    int32_t y = X[g][3];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int32_t v = __shfl_up_sync(FULL, y, d);
+      if (lane >= d) y = maxs(y, v + d * 4 * E);
+    }
+    pre[g] = __shfl_up_sync(FULL, y, 1);
+    if (lane == 0) pre[g] = BELOW;
   }
-  int32_t cin = __shfl_up_sync(FULL, y, 1);
-  cin = lane == 0 ? NEG32 : maxs(cin, NEG32 + C * lane * E);
+  // chain the stripes: carry = I at the stripe's first column (NEG32 at the
+  // band start); each lane's carried-in state is max(pre, carry shifted)
+  int32_t cin[G];
+  int32_t carry = NEG32;
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    cin[g] = maxs(pre[g], carry + 4 * lane * E);
+    carry = __shfl_sync(FULL, maxs(cin[g] + 4 * E, X[g][3]), 31);
+  }
   __syncwarp();  // every predecessor read of the ring precedes this row's writes
-  if (j0 < stop) {
-    const int o = C * lane;
 #pragma unroll
-    for (int k0 = 0; k0 < C; k0 += 4) {
-      if (j0 + k0 < stop) {
-        int32_t iv[4], mv[4];
+  for (int g = 0; g < G; ++g) {
+    const int j0 = start + 128 * g + 4 * lane;
+    if (j0 < stop) {
+      int32_t iv[4], mv[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int k = k0 + q;
-          iv[q] = k == 0 ? cin : maxs(X[k - 1], cin + k * E);
-          mv[q] = maxs(Mx[k], iv[q]);
-          const int j = j0 + k;
-          sm->ring_m[out_slot][j & (RING_W - 1)] = mv[q];
-          sm->ring_d[out_slot][j & (RING_W - 1)] = Dx[k];
-          if (adapt && mv[q] > bestv) {
-            bestv = mv[q];
-            bestj = j;
-          }
+      for (int k = 0; k < 4; ++k) {
+        iv[k] = k == 0 ? cin[g] : maxs(X[g][k - 1], cin[g] + k * E);
+        mv[k] = maxs(Mx[g][k], iv[k]);
+        if (adapt && mv[k] > bestv) {
+          bestv = mv[k];
+          bestj = j0 + k;
         }
-        *reinterpret_cast<int4 *>(R + o + k0) = make_int4(mv[0], mv[1], mv[2], mv[3]);
-        *reinterpret_cast<int4 *>(R + len + o + k0) = make_int4(Dx[k0], Dx[k0 + 1], Dx[k0 + 2], Dx[k0 + 3]);
-        *reinterpret_cast<int4 *>(R + 2 * len + o + k0) = make_int4(iv[0], iv[1], iv[2], iv[3]);
       }
+      const int o = j0 - start;
+      const int x = ring_at(pos_i, start, j0);
+      *reinterpret_cast<int4 *>(sm->ring_m + x) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+      *reinterpret_cast<int4 *>(sm->ring_d + x) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
+      *reinterpret_cast<int4 *>(R + o) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+      *reinterpret_cast<int4 *>(R + len + o) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
+      *reinterpret_cast<int4 *>(R + 2 * len + o) = make_int4(iv[0], iv[1], iv[2], iv[3]);
     }
   }
 }
 
-// Dispatches one int32 row to the blocked tile of the right width.
-__device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_t *R, const int32_t *seq,
+// Dispatches one int32 row to the striped tile of the right width.
+__device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                             const int32_t *mrow, int32_t E, int32_t O, unsigned vmask, int ps,
-                                            int pl, int slot, const int32_t *g, WarpSmem *sm, int out_slot,
-                                            bool adapt, int32_t &bv, int &bj) {
+                                            int pl, int pos, const int32_t *g, WarpSmem *sm, int pos_i, bool adapt,
+                                            int32_t &bv, int &bj) {
   if (len <= 128)
-    dp_row_blocked<4>(lane, start, len, R, seq, mrow, E, O, vmask, ps, pl, slot, g, sm, out_slot, adapt, bv, bj);
+    dp_row_striped<1>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
   else if (len <= 256)
-    dp_row_blocked<8>(lane, start, len, R, seq, mrow, E, O, vmask, ps, pl, slot, g, sm, out_slot, adapt, bv, bj);
+    dp_row_striped<2>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
+  else if (len <= 384)
+    dp_row_striped<3>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
   else
-    dp_row_blocked<16>(lane, start, len, R, seq, mrow, E, O, vmask, ps, pl, slot, g, sm, out_slot, adapt, bv, bj);
+    dp_row_striped<4>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
+}
+
+// Ring entry of a predecessor row's first column (arena offset `po`) while
+// row `off` is computed, or -1 when the row's states are no longer (or were
+// never) in the ring: intact while the rows written after it hold at most
+// RING_CAP entries. Arena offsets are 3x the cumulative band length.
+__device__ __forceinline__ int ring_pos(int64_t po, int64_t off, int64_t ring_floor) {
+  if (po < ring_floor || off - po > 3 * int64_t(RING_CAP)) return -1;
+  return int((po / 3) % RING_CAP);
+}
+
+// Copies row 0 (arena offset 0, computed serially) into the ring; returns the
+// ring floor (1 when the row is too wide to enter it).
+template <typename S>
+__device__ inline int64_t ring_put_row0(WarpSmem *sm, const S *A, int len) {
+  const int lane = threadIdx.x & 31;
+  if (len > RING_MAX_LEN) return 1;
+  for (int c = lane; c < len; c += 32) {
+    sm->ring_m[c] = int32_t(A[c]);
+    sm->ring_d[c] = int32_t(A[len + c]);
+  }
+  __syncwarp();
+  return 0;
 }
 
 // One row by the generic interleaved loop (int64 kernel, rows wider than
-// RING_W, or more than 32 predecessors): 32-column chunks, predecessor rows
+// RING_MAX_LEN, or more than 32 predecessors): 32-column chunks, predecessor rows
 // from the arena, a warp-shuffle scan per chunk with a serial carry.
 template <typename S>
 __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *R, const S *A, const Scratch &s,
@@ -885,6 +1277,24 @@ __device__ __forceinline__ void dp_row0(S *R, int len, S s00, S E, S O) {
   }
 }
 
+// Per predecessor entry: (row, band start, band length, edge weight) and the
+// row's arena offset, once every row's band is known (warp-wide).
+__device__ inline void fill_pmeta(Scratch &s, int n) {
+  const int lane = threadIdx.x & 31;
+  const int etot = s.pred_start[n - 1] + s.pred_cnt[n - 1];
+  for (int e = lane; e < etot; e += 32) {
+    const int2 pr = s.pred[e];
+    if (pr.x >= 0) {
+      s.pmeta[e] = make_int4(pr.x, s.row_start[pr.x], s.row_len[pr.x], pr.y);
+      s.pmeta_off[e] = s.row_off[pr.x];
+    } else {
+      s.pmeta[e] = make_int4(-1, 0, 0, 0);
+      s.pmeta_off[e] = 0;
+    }
+  }
+  __syncwarp();
+}
+
 // One DP kernel invocation (poa_simd_arena, align.rs:588-911, or
 // poa_scalar_i64, align.rs:913-1162) by a whole warp.
 template <typename S>
@@ -901,8 +1311,13 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   if (m > INT32_MAX) return ST_COORD_LIMITS;
   const int64_t padded = (m / 8 + 1) * 8;
   if (!carve_scratch(arena, arena_bytes, n, J->n_edges, padded, m + 1, s)) return ST_ARENA_FULL;
-  for (int64_t c = lane; c < padded; c += 32)
-    s.seq[c] = (c == 0 || c > qlen) ? P.unknown : int(P.encode[query[c - 1]]);
+  // the byte copy the striped rows read: shared memory when it fits
+  uint8_t *q8 = (sm && padded + 4 <= SEQ_SMEM) ? sm->seq8 : s.seq8;
+  for (int64_t c = lane; c < padded + 4; c += 32) {
+    const int code = (c == 0 || c > qlen) ? P.unknown : int(P.encode[query[c - 1]]);
+    if (c < padded) s.seq[c] = code;
+    q8[c] = uint8_t(code);
+  }
   const bool adaptive = adaptive_arg || P.adaptive;
   uint64_t bandu = band_b + (f == 0 ? 0 : uint64_t(m) / f);
   if (bandu < band_b) bandu = UINT64_MAX;
@@ -929,8 +1344,9 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   uint64_t row_cells = 0;
   constexpr bool kFastType = sizeof(S) == 4;
   const bool smem_matrix = P.sigma * P.sigma <= SMEM_MATRIX;
+  // ring entries of rows before ring_floor (an arena offset) are not valid
+  int64_t ring_floor = 0;
   if (sm) {
-    if (lane < RING_ROWS) sm->ring_row[lane] = -1;
     if (smem_matrix)
       for (int k = lane; k < P.sigma * P.sigma; k += 32) sm->matrix[k] = P.matrix[k];
   }
@@ -1000,20 +1416,10 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     }
     if (tot > cap) return ST_ARENA_FULL;
     __syncwarp();
-    const int etot = s.pred_start[n - 1] + s.pred_cnt[n - 1];
-    for (int e = lane; e < etot; e += 32) {
-      const int p = s.pred[e].x;
-      if (p >= 0) {
-        s.pmeta[e] = make_int4(p, s.row_start[p], s.row_len[p], 0);
-        s.pmeta_off[e] = s.row_off[p];
-      } else {
-        s.pmeta[e] = make_int4(-1, 0, 0, 0);
-        s.pmeta_off[e] = 0;
-      }
-    }
-    __syncwarp();
+    fill_pmeta(s, n);
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
     __syncwarp();
+    if (kFastType && sm) ring_floor = ring_put_row0(sm, A, s.row_len[0]);
     // rows 1..n-1, software-pipelined: row i+2's descriptor and row i+1's
     // predecessor metadata are loaded while row i computes
     auto desc = [&](int r) { return make_int4(s.row_start[r], s.row_len[r], s.pred_start[r], s.pred_cnt[r]); };
@@ -1050,24 +1456,20 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
       const int start = d.x, len = d.y, pb = d.z, pc = d.w;
       if (len == 0) continue;
       S *R = A + off;
-      if (kFastType && sm && len <= RING_W && pc <= 32) {
-        const int p = mt.x;
-        const bool ok = p >= 0 && mt.z > 0;
-        const int sl = p >= 0 ? p % RING_ROWS : 0;
-        const int my_slot = (ok && sm->ring_row[sl] == p) ? sl : -1;
+      if (kFastType && sm && len <= RING_MAX_LEN && pc <= 32) {
+        const bool ok = mt.x >= 0 && mt.z > 0;
+        const int my_pos = ok ? ring_pos(mo, off, ring_floor) : -1;
         const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + mo;
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
-        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), s.seq, mrow, int32_t(E), int32_t(O), vmask,
-                    mt.y, mt.z, my_slot, my_g, sm, i % RING_ROWS, false, bv, bj);
-        __syncwarp();
-        if (lane == 0) sm->ring_row[i % RING_ROWS] = i;
+        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask, mt.y,
+                    mt.z, my_pos, my_g, sm, int((off / 3) % RING_CAP), false, bv, bj);
         __syncwarp();
         continue;
       }
-      if (sm && lane == 0) sm->ring_row[i % RING_ROWS] = -1;
+      ring_floor = off + 1;  // this row does not enter the ring
       S bv = ScoreTraits<S>::LOWEST;
       int bj = INT32_MAX;
       dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, false, bv, bj);
@@ -1110,6 +1512,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         s.row_off[i] = off;
       }
       S *R = A + off;
+      if (lane == 0) s.row_base[i] = (i == n - 1) ? P.unknown : int(J->base[J->rank_to_node[beg + i]]);
       if (i == 0) {
         if (start != 0) {
           cells->cells += row_cells;
@@ -1118,6 +1521,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         }
         if (lane == 0) dp_row0<S>(R, len, s00, E, O);
         __syncwarp();
+        if (kFastType && sm) ring_floor = ring_put_row0(sm, A, len);
         continue;
       }
       const int node = J->rank_to_node[beg + i];
@@ -1125,8 +1529,8 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
       const int pb = s.pred_start[i], pc = s.pred_cnt[i];
       S bestv = ScoreTraits<S>::LOWEST;
       int bestj = INT32_MAX;
-      if (kFastType && sm && len <= RING_W && pc <= 32) {
-        int my_ps = 0, my_pl = 0, my_slot = -1;
+      if (kFastType && sm && len <= RING_MAX_LEN && pc <= 32) {
+        int my_ps = 0, my_pl = 0, my_pos = -1;
         const int32_t *my_g = nullptr;
         bool ok = false;
         if (lane < pc) {
@@ -1134,24 +1538,22 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
           if (p >= 0) {
             my_ps = s.row_start[p];
             my_pl = s.row_len[p];
-            my_g = reinterpret_cast<const int32_t *>(A) + s.row_off[p];
-            const int sl = p % RING_ROWS;
-            my_slot = sm->ring_row[sl] == p ? sl : -1;
+            const int64_t po = s.row_off[p];
+            my_g = reinterpret_cast<const int32_t *>(A) + po;
             ok = my_pl > 0;
+            if (ok) my_pos = ring_pos(po, off, ring_floor);
           }
         }
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
-        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), s.seq, mrow, int32_t(E), int32_t(O), vmask,
-                    my_ps, my_pl, my_slot, my_g, sm, i % RING_ROWS, true, bv, bj);
-        __syncwarp();
-        if (lane == 0) sm->ring_row[i % RING_ROWS] = i;
+        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask, my_ps,
+                    my_pl, my_pos, my_g, sm, int((off / 3) % RING_CAP), true, bv, bj);
         bestv = S(bv);
         bestj = bj;
       } else {
-        if (sm && lane == 0) sm->ring_row[i % RING_ROWS] = -1;
+        ring_floor = off + 1;  // this row does not enter the ring
         dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, true, bestv, bestj);
       }
       __syncwarp();
@@ -1172,9 +1574,11 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   }
   cells->cells += row_cells;
   cells->dp_bytes += row_cells * 3 * sizeof(S);
-  if (lane == 0) st = traceback<S>(J, P, s, A, beg, n, m, n_items);
-  st = __shfl_sync(FULL, st, 0);
-  *n_items = __shfl_sync(FULL, *n_items, 0);
+  if (do_adapt) {
+    __syncwarp();
+    fill_pmeta(s, n);
+  }
+  st = traceback<S>(J, P, s, A, beg, n, m, (sm && smem_matrix) ? sm->matrix : P.matrix, n_items);
   return st;
 }
 
@@ -1273,31 +1677,58 @@ __device__ inline bool reorder_incremental(Job *J, const int4 *items, int n_item
     }
   }
   __syncwarp();
+  // new ranks, four 32-row groups per step so their loads overlap
+  constexpr int U = 4;
   int shift = 0;
-  for (int r0 = 0; r0 < n_old; r0 += 32) {
-    const int r = r0 + lane;
-    const int a = r < n_old ? add[r] : 0;
-    int inc = a;
+  for (int r0 = 0; r0 < n_old; r0 += 32 * U) {
+    int a[U], node[U], inc[U];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int v = __shfl_up_sync(FULL, inc, d);
-      if (lane >= d) inc += v;
+    for (int u = 0; u < U; ++u) {
+      const int r = r0 + 32 * u + lane;
+      a[u] = r < n_old ? add[r] : 0;
+      node[u] = r < n_old ? J->rank_to_node[r] : 0;
     }
-    if (r < n_old) {
-      const int node = J->rank_to_node[r];
-      const int nr = r + shift + inc - a;
-      nr2n[nr] = node;
-      J->rank[node] = nr;
-      for (int k = 0; k < a; ++k) {
-        const int id = first[r] + k;
-        nr2n[nr + 1 + k] = id;
-        J->rank[id] = nr + 1 + k;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      inc[u] = a[u];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(FULL, inc[u], d);
+        if (lane >= d) inc[u] += v;
       }
     }
-    shift += __shfl_sync(FULL, inc, 31);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int r = r0 + 32 * u + lane;
+      if (r < n_old) {
+        const int nr = r + shift + inc[u] - a[u];
+        nr2n[nr] = node[u];
+        J->rank[node[u]] = nr;
+        if (a[u] > 0) {
+          const int f = first[r];
+          for (int k = 0; k < a[u]; ++k) {
+            nr2n[nr + 1 + k] = f + k;
+            J->rank[f + k] = nr + 1 + k;
+          }
+        }
+      }
+      shift += __shfl_sync(FULL, inc[u], 31);
+    }
   }
   __syncwarp();
-  for (int r = lane; r < n_new; r += 32) J->rank_to_node[r] = nr2n[r];
+  for (int r0 = 0; r0 < n_new; r0 += 32 * U) {
+    int v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int r = r0 + 32 * u + lane;
+      v[u] = r < n_new ? nr2n[r] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int r = r0 + 32 * u + lane;
+      if (r < n_new) J->rank_to_node[r] = v[u];
+    }
+  }
   if (lane == 0) J->n_rank = n_new;
   __syncwarp();
   return true;
@@ -1332,8 +1763,10 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, sm);
   if (st != ST_OK) return st;
   const int n_old = J->n_nodes;
-  if (lane == 0) st = add_path(J, P, r, s.items, n_items);
-  st = __shfl_sync(FULL, st, 0);
+  if (!add_path_warp(J, P, r, s.items, n_items, &st)) {
+    if (lane == 0) st = add_path(J, P, r, s.items, n_items);
+    st = __shfl_sync(FULL, st, 0);
+  }
   __syncwarp();
   if (st != ST_OK) return st;
   // order-free reads (static band, no seeding) keep a spliced order; the

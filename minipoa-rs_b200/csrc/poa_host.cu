@@ -565,7 +565,7 @@ struct poa_batch {
     ctx->dfree(storage, storage_bytes);
     ctx->dfree(d_jobs, jobs.size() * sizeof(Job));
     ctx->dfree(d_order, order.size() * 4 + 4);
-    ctx->dfree(d_queue, 16);
+    ctx->dfree(d_queue, sched_words(jobs.size()) * 4);
     ctx->dfree(arenas, size_t(arena_pool));
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -587,6 +587,15 @@ struct poa_batch {
     std::vector<int64_t> off(ids.size() + 1, 0);
     for (size_t k = 0; k < ids.size(); ++k) off[k + 1] = off[k] + packed_words(jobs[size_t(ids[k])], sigma);
     const size_t words = size_t(off.back());
+    // The DP arena pool takes what the budget leaves after a run; when the
+    // packed graphs do not fit beside it, the pool is released (the next run
+    // allocates it again).
+    const uint64_t need = words * 4 + 16 + off.size() * 8 + ids.size() * 4 + 4 + 3 * 256;
+    if (arenas && ctx->allocated + need > ctx->budget) {
+      ctx->dfree(arenas, size_t(arena_pool));
+      arenas = nullptr;
+      arena_pool = 0;
+    }
     int32_t *d_out = (int32_t *)ctx->dalloc(words * 4 + 16);
     int64_t *d_off = (int64_t *)ctx->dalloc(off.size() * 8);
     int32_t *d_ids = (int32_t *)ctx->dalloc(ids.size() * 4 + 4);
@@ -1004,7 +1013,7 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     std::iota(b->order.begin(), b->order.end(), 0);
     std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return est[a] > est[c]; });
     b->d_order = (int32_t *)ctx->dalloc(b->order.size() * 4 + 4);
-    b->d_queue = (int32_t *)ctx->dalloc(16);
+    b->d_queue = (int32_t *)ctx->dalloc(sched_words(b->jobs.size()) * 4);
     CK(cudaEventCreate(&b->e0));
     CK(cudaEventCreate(&b->e1));
     CK(cudaEventCreate(&b->k0));
@@ -1033,7 +1042,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
       b->arena_pool = pool;
     }
     const int sms = ctx->sm_count;
-    int wps = b->warps_per_sm > 0 ? b->warps_per_sm : 16;
+    int wps = b->warps_per_sm > 0 ? b->warps_per_sm : batch_resident_warps_per_sm();
     int passes = 0, launches = 0;
     double kernel_ms = 0;
     CK(cudaEventRecord(b->e0, ctx->stream));
@@ -1050,9 +1059,10 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
           slot_bytes = std::min<int64_t>(int64_t(b->slot_bytes_override), slot_bytes);
         if (passes == 0) slots_first = int(slots);
         CK(cudaMemcpyAsync(b->d_order, pending.data(), pending.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemsetAsync(b->d_queue, 0, 4, ctx->stream));
+        CK(cudaMemsetAsync(b->d_queue, 0, sched_words(pending.size()) * 4, ctx->stream));
         CK(cudaEventRecord(b->k0, ctx->stream));
-        CK(launch_batch(b->d_jobs, b->d_order, int(pending.size()), b->d_queue, b->P, b->arenas, slot_bytes,
+        CK(launch_batch(b->d_jobs, b->d_order, int(pending.size()), b->d_queue, ctx->sm_count, b->P, b->arenas,
+                        slot_bytes,
                         int(slots), ctx->stream));
         CK(cudaEventRecord(b->k1, ctx->stream));
         ++launches;

@@ -9,8 +9,13 @@
 namespace poa {
 
 // Launchers (poa_kernels.cu). All are asynchronous on `stream`.
-cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *queue, const DevParams &P,
-                         char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream);
+// `sched` holds sched_words(n_jobs) zeroed int32 words: the queue head, the
+// per-SM and per-level counters that spread the first jobs over the SMs, and
+// one claim flag per queue position.
+constexpr int SCHED_SM_SLOTS = 512, SCHED_LEVELS = 64;
+inline size_t sched_words(size_t n_jobs) { return 4 + SCHED_SM_SLOTS + SCHED_LEVELS + n_jobs; }
+cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
+                         const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream);
 cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,
                                cudaStream_t stream);
 cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *reads,
@@ -26,5 +31,7 @@ cudaError_t launch_add_edge(Job *job_dev, int from, int to, cudaStream_t stream)
 cudaError_t launch_toposort(Job *job_dev, char *arena, int64_t bytes, cudaStream_t stream);
 cudaError_t launch_reset(Job *jobs_dev, int n_jobs, int sigma, int unknown, cudaStream_t stream);
 int kernel_launches_per_batch();
+// Warps of the batched kernel resident on one SM (its blocks per SM x warps per block).
+int batch_resident_warps_per_sm();
 
 }  // namespace poa

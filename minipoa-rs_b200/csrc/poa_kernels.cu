@@ -7,6 +7,11 @@
 namespace poa {
 
 constexpr int WARPS_PER_BLOCK = 4;
+// Two 4-warp blocks of the batched kernel fit one SM's 228 KB of shared
+// memory (1 KB of it is reserved per block), matching __launch_bounds__.
+constexpr int BLOCKS_PER_SM = 2;
+static_assert(BLOCKS_PER_SM * (WARPS_PER_BLOCK * sizeof(WarpSmem) + 1024) <= 228 * 1024,
+              "WarpSmem too large for the blocks per SM");
 
 __device__ __forceinline__ WarpSmem *warp_smem() {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -16,9 +21,13 @@ __device__ __forceinline__ WarpSmem *warp_smem() {
 // Persistent batched kernel: each warp takes jobs from a size-ordered queue
 // (largest first) and runs their remaining reads. A job that outgrows the
 // warp's DP arena parks at its current read (graph untouched) for a later
-// pass with larger arenas.
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3)
-    k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *queue, DevParams P, char *arenas,
+// pass with larger arenas. The first job of every warp is placed so that the
+// largest jobs land on different SMs: the k-th warp to start on an SM takes
+// one of the positions [k * num_sms, (k + 1) * num_sms), in the order the SMs
+// reach that level; every later job comes from the shared queue, and a claim
+// flag per position makes each job run exactly once.
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
+    k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *sched, int num_sms, DevParams P, char *arenas,
             int64_t slot_bytes, int slots) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -26,11 +35,35 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3)
   if (warp >= slots) return;
   char *arena = arenas + warp * slot_bytes;
   WarpSmem *sm = warp_smem();
+  int32_t *queue = sched;
+  int32_t *sm_count = sched + 4;
+  int32_t *level_count = sm_count + SCHED_SM_SLOTS;
+  int32_t *claim = level_count + SCHED_LEVELS;
+  int first = -1;
+  if (lane == 0) {
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (smid < unsigned(SCHED_SM_SLOTS)) {
+      const int level = atomicAdd(&sm_count[smid], 1);
+      if (level < SCHED_LEVELS) {
+        const int64_t p0 = int64_t(level) * num_sms + atomicAdd(&level_count[level], 1);
+        if (p0 < n_jobs && atomicExch(&claim[p0], 1) == 0) first = int(p0);
+      }
+    }
+  }
+  first = __shfl_sync(FULL, first, 0);
   for (;;) {
-    int q = 0;
-    if (lane == 0) q = atomicAdd(queue, 1);
-    q = __shfl_sync(FULL, q, 0);
-    if (q >= n_jobs) break;
+    int q = first;
+    first = -1;
+    if (q < 0) {
+      if (lane == 0) {
+        do {
+          q = atomicAdd(queue, 1);
+        } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
+      }
+      q = __shfl_sync(FULL, q, 0);
+      if (q >= n_jobs) break;
+    }
     Job *J = jobs + order[q];
     const int n_reads = J->n_reads;
     int32_t st = ST_OK;
@@ -113,7 +146,9 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
 }
 
 __global__ void k_add_path(Job *J, DevParams P, int seq_id, int4 *items, int n) {
-  if (threadIdx.x == 0) J->status = add_path(J, P, seq_id, items, n);
+  int32_t st = ST_OK;
+  if (!add_path_warp(J, P, seq_id, items, n, &st) && threadIdx.x == 0) st = add_path(J, P, seq_id, items, n);
+  if (threadIdx.x == 0) J->status = st;
 }
 
 __global__ void k_add_node(Job *J, int sigma, int base) {
@@ -174,8 +209,8 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   J->order_exact = 1;
 }
 
-cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *queue, const DevParams &P,
-                         char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
+cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
+                         const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
   const int blocks = (slots + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
   const size_t smem = WARPS_PER_BLOCK * sizeof(WarpSmem);
   static bool attr = false;
@@ -184,8 +219,8 @@ cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, 
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_batch<<<blocks, WARPS_PER_BLOCK * 32, smem, stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, queue, P,
-                                                          arenas, slot_bytes, slots);
+  k_batch<<<blocks, WARPS_PER_BLOCK * 32, smem, stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, sched,
+                                                          num_sms, P, arenas, slot_bytes, slots);
   return cudaGetLastError();
 }
 
@@ -237,5 +272,7 @@ cudaError_t launch_reset(Job *jobs_dev, int n_jobs, int sigma, int unknown, cuda
 }
 
 int kernel_launches_per_batch() { return 1; }
+
+int batch_resident_warps_per_sm() { return BLOCKS_PER_SM * WARPS_PER_BLOCK; }
 
 }  // namespace poa
