@@ -9,7 +9,7 @@
  *
  * Each entry point names the reference item it replaces (paths inside the
  * minipoa-rs project). The reference is a Rust library with no FFI of its
- * own; INTEGRATION.md shows the extern "C" block a Rust FFI crate binds.
+ * own; a Rust FFI crate binds these declarations in an extern "C" block.
  *
  * Conventions: every call returns int status (POA_OK = 0); on failure
  * poa_last_error(ctx) gives the reference's error text. Buffers passed in are
