@@ -118,6 +118,10 @@ struct Scratch {
   int32_t *row_base;   // base code a row scores with (N for the last row)
   int4 *pmeta;         // per pred entry: (row, band start, band length, -)
   int64_t *pmeta_off;  // per pred entry: the predecessor row's arena offset
+  int4 *plan;          // static band, per row: (band start, band length, pred_start, pred_cnt)
+  int4 *plan2;         // static band, per row: (arena offset lo, hi, base code, ring entry)
+  int4 *pmeta2;        // static band, per pred entry: (ring entry or -1, arena offset lo, hi, -)
+  int32_t *nf;         // static band, per row: rows before it that did not go through the ring
   int32_t *seq;        // encoded, padded query
   uint8_t *seq8;       // the same, one byte per column (when it does not fit shared memory)
   int4 *items;         // alignment result (node, base, aligned, resolved id)
@@ -161,6 +165,10 @@ __device__ inline bool carve_scratch(char *arena, int64_t bytes, int n, int e, i
   s.row_base = (int32_t *)take(N * 4);
   s.pmeta = (int4 *)take(int64_t(e + 1) * 16);
   s.pmeta_off = (int64_t *)take(int64_t(e + 1) * 8);
+  s.plan = (int4 *)take(N * 16);
+  s.plan2 = (int4 *)take(N * 16);
+  s.pmeta2 = (int4 *)take(int64_t(e + 1) * 16);
+  s.nf = (int32_t *)take(N * 4);
   s.seq = (int32_t *)take((padded + 32) * 4);
   s.seq8 = (uint8_t *)take(padded + 32);
   s.items = (int4 *)take((n_items + 1) * 16);
@@ -1056,12 +1064,14 @@ __device__ __forceinline__ int ring_at(int pos, int start, int j) {
 // columns, a warp max-plus scan (shift 4E per lane) carries the insertion
 // state across the lanes of a stripe, and the stripes chain their carries.
 // All identities are exact in integers: I[j+1] = max(I[j] + E, md[j] + O)
-// with I[start] = NEG32.
-template <int G>
+// with I[start] = NEG32. The stripe loops are branch-free (loads go to a
+// clamped, in-bounds column and the value is then selected) so the compiler
+// can overlap the stripes' dependency chains.
+template <int G, bool ADAPT>
 __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                                const int32_t *mrow, int32_t E, int32_t O, unsigned vmask,
                                                int my_ps, int my_pl, int my_pos, const int32_t *my_g,
-                                               WarpSmem *sm, int pos_i, bool adapt, int32_t &bestv, int &bestj) {
+                                               WarpSmem *sm, int pos_i, int32_t &bestv, int &bestj) {
   const int stop = start + len;
   int32_t Mx[G][4], Dx[G][4];
 #pragma unroll
@@ -1078,51 +1088,67 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
     const int pl = __shfl_sync(FULL, my_pl, t);
     const int pos = __shfl_sync(FULL, my_pos, t);
     const int32_t *gp = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
+    int4 m4[G], d4[G];
+    int32_t prev[G];
+    bool in[G];
+    if (pos >= 0) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int j0 = start + 128 * g + 4 * lane;
+        in[g] = j0 < stop && j0 >= ps && j0 < ps + pl;
+        const int x = ring_at(pos, ps, in[g] ? j0 : ps);
+        m4[g] = *reinterpret_cast<const int4 *>(sm->ring_m + x);
+        d4[g] = *reinterpret_cast<const int4 *>(sm->ring_d + x);
+        prev[g] = sm->ring_m[x == 0 ? RING_CAP - 1 : x - 1];
+      }
+    } else {
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int j0 = start + 128 * g + 4 * lane;
+        in[g] = j0 < stop && j0 >= ps && j0 < ps + pl;
+        const int c = in[g] ? j0 - ps : 0;
+        m4[g] = *reinterpret_cast<const int4 *>(gp + c);
+        d4[g] = *reinterpret_cast<const int4 *>(gp + pl + c);
+        prev[g] = gp[c > 0 ? c - 1 : 0];
+      }
+    }
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       const int j0 = start + 128 * g + 4 * lane;
-      if (j0 < stop && j0 >= ps && j0 < ps + pl) {
-        int4 m4, d4;
-        int32_t prev = NEG32;
-        if (pos >= 0) {
-          const int x = ring_at(pos, ps, j0);
-          m4 = *reinterpret_cast<const int4 *>(sm->ring_m + x);
-          d4 = *reinterpret_cast<const int4 *>(sm->ring_d + x);
-          if (j0 > ps) prev = sm->ring_m[x == 0 ? RING_CAP - 1 : x - 1];
-        } else {
-          m4 = *reinterpret_cast<const int4 *>(gp + (j0 - ps));
-          d4 = *reinterpret_cast<const int4 *>(gp + pl + (j0 - ps));
-          if (j0 > ps) prev = gp[j0 - ps - 1];
-        }
-        Mx[g][0] = maxs(Mx[g][0], prev);
-        Mx[g][1] = maxs(Mx[g][1], m4.x);
-        Mx[g][2] = maxs(Mx[g][2], m4.y);
-        Mx[g][3] = maxs(Mx[g][3], m4.z);
-        Dx[g][0] = maxs(Dx[g][0], maxs(d4.x + E, m4.x + O));
-        Dx[g][1] = maxs(Dx[g][1], maxs(d4.y + E, m4.y + O));
-        Dx[g][2] = maxs(Dx[g][2], maxs(d4.z + E, m4.z + O));
-        Dx[g][3] = maxs(Dx[g][3], maxs(d4.w + E, m4.w + O));
+      const int32_t pv = j0 > ps ? prev[g] : NEG32;
+      if (in[g]) {
+        Mx[g][0] = maxs(Mx[g][0], pv);
+        Mx[g][1] = maxs(Mx[g][1], m4[g].x);
+        Mx[g][2] = maxs(Mx[g][2], m4[g].y);
+        Mx[g][3] = maxs(Mx[g][3], m4[g].z);
+        Dx[g][0] = maxs(Dx[g][0], maxs(d4[g].x + E, m4[g].x + O));
+        Dx[g][1] = maxs(Dx[g][1], maxs(d4[g].y + E, m4[g].y + O));
+        Dx[g][2] = maxs(Dx[g][2], maxs(d4[g].z + E, m4[g].z + O));
+        Dx[g][3] = maxs(Dx[g][3], maxs(d4[g].w + E, m4[g].w + O));
       }
     }
   }
   // md, the in-lane scan x[k] = max over k' <= k of md[k'] + O + (k-k')E, and
   // per stripe the warp scan of the lane aggregates: pre[g] = the insertion
   // state entering the lane's first column from the lanes before it (without
-  // the stripe's own carry; a value below every reachable state for lane 0)
+  // the stripe's own carry; a value below every reachable state for lane 0).
+  // Columns past the band read the band's last word and are never stored.
   constexpr int32_t BELOW = INT32_MIN / 2;
   int32_t X[G][4], pre[G];
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     const int j0 = start + 128 * g + 4 * lane;
-    uint32_t bw = 0;
-    if (j0 < stop) bw = *reinterpret_cast<const uint32_t *>(seq8 + j0);
+    const uint32_t bw = *reinterpret_cast<const uint32_t *>(seq8 + min(j0, stop - 4));
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const int32_t prof = j0 < stop ? mrow[(bw >> (8 * k)) & 0xff] : 0;
+      const int32_t prof = mrow[(bw >> (8 * k)) & 0xff];
       Mx[g][k] = maxs(Mx[g][k] + prof, Dx[g][k]);  // Mx now holds md
       X[g][k] = Mx[g][k] + O;
       if (k > 0) X[g][k] = maxs(X[g][k], X[g][k - 1] + E);
     }
+  }
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
     int32_t y = X[g][3];
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -1139,22 +1165,26 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     cin[g] = maxs(pre[g], carry + 4 * lane * E);
-    carry = __shfl_sync(FULL, maxs(cin[g] + 4 * E, X[g][3]), 31);
+    if (g + 1 < G) carry = __shfl_sync(FULL, maxs(cin[g] + 4 * E, X[g][3]), 31);
   }
   __syncwarp();  // every predecessor read of the ring precedes this row's writes
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     const int j0 = start + 128 * g + 4 * lane;
-    if (j0 < stop) {
-      int32_t iv[4], mv[4];
+    int32_t iv[4], mv[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        iv[k] = k == 0 ? cin[g] : maxs(X[g][k - 1], cin[g] + k * E);
-        mv[k] = maxs(Mx[g][k], iv[k]);
-        if (adapt && mv[k] > bestv) {
-          bestv = mv[k];
-          bestj = j0 + k;
-        }
+    for (int k = 0; k < 4; ++k) {
+      iv[k] = k == 0 ? cin[g] : maxs(X[g][k - 1], cin[g] + k * E);
+      mv[k] = maxs(Mx[g][k], iv[k]);
+    }
+    if (j0 < stop) {
+      if (ADAPT) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (mv[k] > bestv) {
+            bestv = mv[k];
+            bestj = j0 + k;
+          }
       }
       const int o = j0 - start;
       const int x = ring_at(pos_i, start, j0);
@@ -1168,18 +1198,19 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
 }
 
 // Dispatches one int32 row to the striped tile of the right width.
+template <bool ADAPT>
 __device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                             const int32_t *mrow, int32_t E, int32_t O, unsigned vmask, int ps,
-                                            int pl, int pos, const int32_t *g, WarpSmem *sm, int pos_i, bool adapt,
-                                            int32_t &bv, int &bj) {
+                                            int pl, int pos, const int32_t *g, WarpSmem *sm, int pos_i, int32_t &bv,
+                                            int &bj) {
   if (len <= 128)
-    dp_row_striped<1>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
+    dp_row_striped<1, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
   else if (len <= 256)
-    dp_row_striped<2>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
+    dp_row_striped<2, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
   else if (len <= 384)
-    dp_row_striped<3>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
+    dp_row_striped<3, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
   else
-    dp_row_striped<4>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, adapt, bv, bj);
+    dp_row_striped<4, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
 }
 
 // Ring entry of a predecessor row's first column (arena offset `po`) while
@@ -1275,6 +1306,56 @@ __device__ __forceinline__ void dp_row0(S *R, int len, S s00, S E, S O) {
     R[2 * len + c] = ins;
     R[c] = maxs<S>(R[c], ins);
   }
+}
+
+// A 16-byte load issued where it is written: the DP loop loads the next rows'
+// plan while the current row computes, and a volatile load keeps the
+// compiler from sinking it to its use.
+__device__ __forceinline__ int4 ld_early(const int4 *p) {
+  int4 v;
+  asm volatile("ld.global.v4.s32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+
+// Static-band row plan (warp-wide), after fill_pmeta: per row its band,
+// predecessor list, arena offset, base code and ring entry, and per
+// predecessor entry where its states are: the ring entry of the
+// predecessor's first column when its states are still in the ring (the
+// predecessor and every row after it went through the ring, and at most
+// RING_CAP entries were written since), else -1, plus its arena offset. A row
+// goes through the ring when `ring` is set, its band is at most RING_MAX_LEN
+// and it has at most 32 predecessors (row 0: when its band fits).
+__device__ inline void plan_rows(Scratch &s, int n, bool ring) {
+  const int lane = threadIdx.x & 31;
+  int carry = 0;  // rows before this block that did not go through the ring
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    const int i = i0 + lane;
+    bool fast = true;
+    if (i < n) {
+      const int len = s.row_len[i], pc = s.pred_cnt[i];
+      fast = ring && len <= RING_MAX_LEN && (i == 0 || pc <= 32);
+      const int64_t off = s.row_off[i];
+      s.plan[i] = make_int4(s.row_start[i], len, s.pred_start[i], pc);
+      s.plan2[i] = make_int4(int(uint64_t(off) & 0xffffffffu), int(uint64_t(off) >> 32), s.row_base[i],
+                             int((off / 3) % RING_CAP));
+    }
+    const unsigned slow = __ballot_sync(FULL, i < n && !fast);
+    if (i < n) s.nf[i] = carry + __popc(slow & ((1u << lane) - 1u));  // non-ring rows among 0..i-1
+    carry += __popc(slow);
+  }
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) {
+    const int pb = s.pred_start[i], pc = s.pred_cnt[i], nfi = s.nf[i];
+    const int64_t off = s.row_off[i];
+    for (int t = 0; t < pc; ++t) {
+      const int4 m = s.pmeta[pb + t];
+      const int64_t po = s.pmeta_off[pb + t];
+      int pos = -1;
+      if (m.x >= 0 && m.z > 0 && s.nf[m.x] == nfi && off - po <= 3 * int64_t(RING_CAP)) pos = int((po / 3) % RING_CAP);
+      s.pmeta2[pb + t] = make_int4(pos, int(uint64_t(po) & 0xffffffffu), int(uint64_t(po) >> 32), 0);
+    }
+  }
+  __syncwarp();
 }
 
 // Per predecessor entry: (row, band start, band length, edge weight) and the
@@ -1417,59 +1498,53 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     if (tot > cap) return ST_ARENA_FULL;
     __syncwarp();
     fill_pmeta(s, n);
+    const bool ring = kFastType && sm;
+    plan_rows(s, n, ring);
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
     __syncwarp();
-    if (kFastType && sm) ring_floor = ring_put_row0(sm, A, s.row_len[0]);
-    // rows 1..n-1, software-pipelined: row i+2's descriptor and row i+1's
-    // predecessor metadata are loaded while row i computes
-    auto desc = [&](int r) { return make_int4(s.row_start[r], s.row_len[r], s.pred_start[r], s.pred_cnt[r]); };
-    int4 d1 = n > 1 ? desc(1) : make_int4(0, 0, 0, 0);
-    int4 d2 = n > 2 ? desc(2) : make_int4(0, 0, 0, 0);
-    int64_t o1 = n > 1 ? s.row_off[1] : 0, o2 = n > 2 ? s.row_off[2] : 0;
-    int b1 = n > 1 ? s.row_base[1] : 0, b2 = n > 2 ? s.row_base[2] : 0;
-    int4 m1 = make_int4(-1, 0, 0, 0);
-    int64_t mo1 = 0;
-    if (n > 1 && lane < d1.w) {
-      m1 = s.pmeta[d1.z + lane];
-      mo1 = s.pmeta_off[d1.z + lane];
+    if (ring) ring_put_row0(sm, A, s.row_len[0]);
+    // rows 1..n-1, software-pipelined: row i+2's plan and row i+1's
+    // predecessor entries are loaded while row i computes
+    const int4 zero = make_int4(0, 0, 0, 0), none = make_int4(-1, 0, 0, 0);
+    int4 pa1 = n > 1 ? ld_early(s.plan + 1) : zero, pb1 = n > 1 ? ld_early(s.plan2 + 1) : zero;
+    int4 pa2 = n > 2 ? ld_early(s.plan + 2) : zero, pb2 = n > 2 ? ld_early(s.plan2 + 2) : zero;
+    int4 q1 = none, r1 = zero;
+    if (n > 1 && lane < pa1.w) {
+      q1 = ld_early(s.pmeta + pa1.z + lane);
+      r1 = ld_early(s.pmeta2 + pa1.z + lane);
     }
     for (int i = 1; i < n; ++i) {
-      const int4 d = d1;
-      const int64_t off = o1;
-      const int base = b1;
-      const int4 mt = m1;
-      const int64_t mo = mo1;
-      d1 = d2;
-      o1 = o2;
-      b1 = b2;
-      m1 = make_int4(-1, 0, 0, 0);
-      mo1 = 0;
-      if (i + 1 < n && lane < d1.w) {
-        m1 = s.pmeta[d1.z + lane];
-        mo1 = s.pmeta_off[d1.z + lane];
+      const int4 a = pa1, b = pb1, mt = q1, mr = r1;
+      pa1 = pa2;
+      pb1 = pb2;
+      q1 = none;
+      r1 = zero;
+      if (i + 1 < n && lane < pa1.w) {
+        q1 = ld_early(s.pmeta + pa1.z + lane);
+        r1 = ld_early(s.pmeta2 + pa1.z + lane);
       }
       if (i + 2 < n) {
-        d2 = desc(i + 2);
-        o2 = s.row_off[i + 2];
-        b2 = s.row_base[i + 2];
+        pa2 = ld_early(s.plan + i + 2);
+        pb2 = ld_early(s.plan2 + i + 2);
       }
-      const int start = d.x, len = d.y, pb = d.z, pc = d.w;
+      const int start = a.x, len = a.y, pb = a.z, pc = a.w;
       if (len == 0) continue;
+      const int64_t off = int64_t((uint64_t(uint32_t(b.y)) << 32) | uint32_t(b.x));
+      const int base = b.z;
       S *R = A + off;
-      if (kFastType && sm && len <= RING_MAX_LEN && pc <= 32) {
+      if (ring && len <= RING_MAX_LEN && pc <= 32) {
         const bool ok = mt.x >= 0 && mt.z > 0;
-        const int my_pos = ok ? ring_pos(mo, off, ring_floor) : -1;
+        const int64_t mo = int64_t((uint64_t(uint32_t(mr.z)) << 32) | uint32_t(mr.y));
         const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + mo;
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
-        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask, mt.y,
-                    mt.z, my_pos, my_g, sm, int((off / 3) % RING_CAP), false, bv, bj);
+        dp_row_fast<false>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
+                           mt.y, mt.z, ok ? mr.x : -1, my_g, sm, b.w, bv, bj);
         __syncwarp();
         continue;
       }
-      ring_floor = off + 1;  // this row does not enter the ring
       S bv = ScoreTraits<S>::LOWEST;
       int bj = INT32_MAX;
       dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, false, bv, bj);
@@ -1548,8 +1623,8 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
-        dp_row_fast(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask, my_ps,
-                    my_pl, my_pos, my_g, sm, int((off / 3) % RING_CAP), true, bv, bj);
+        dp_row_fast<true>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
+                          my_ps, my_pl, my_pos, my_g, sm, int((off / 3) % RING_CAP), bv, bj);
         bestv = S(bv);
         bestj = bj;
       } else {
@@ -1622,27 +1697,118 @@ __device__ inline int32_t align_query(Job *J, const DevParams &P, char *arena, i
   return poa_retry(J, P, arena, bytes, 0, 1, q, qlen, P.adaptive != 0, P.b, s, n_items, cells, sm);
 }
 
+// Re-sorts the rank windows of reorder_incremental (warp-wide). spans[k] =
+// (u, v, old rank of u, -): path node u is followed on the path, after the new
+// nodes spliced behind it (add[old rank of u] of them), by v of lower rank.
+// Each window [rank(v), rank(u) + add] is merged with those it overlaps and
+// re-sorted by Kahn's algorithm over the edges inside it. Returns false when a
+// window holds a cycle.
+__device__ inline bool repair_windows(Job *J, int4 *spans, int n_spans, const int32_t *add, int32_t *deg,
+                                      int32_t *stack, int32_t *order) {
+  const int lane = threadIdx.x & 31;
+  // windows in new ranks, sorted by their first rank (lane 0; few per read)
+  if (lane == 0) {
+    for (int k = 0; k < n_spans; ++k) {
+      const int4 sp = spans[k];
+      spans[k] = make_int4(J->rank[sp.y], J->rank[sp.x] + add[sp.z], 0, 0);
+    }
+    for (int k = 1; k < n_spans; ++k) {
+      const int4 x = spans[k];
+      int q = k - 1;
+      while (q >= 0 && spans[q].x > x.x) {
+        spans[q + 1] = spans[q];
+        --q;
+      }
+      spans[q + 1] = x;
+    }
+  }
+  __syncwarp();
+  bool ok = true;
+  int k = 0;
+  while (k < n_spans && ok) {
+    const int lo = spans[k].x;
+    int hi = spans[k].y;
+    ++k;
+    while (k < n_spans && spans[k].x <= hi) {
+      hi = max(hi, spans[k].y);
+      ++k;
+    }
+    const int w = hi - lo + 1;
+    // in-degree from inside the window
+    for (int q = lane; q < w; q += 32) {
+      const int node = J->rank_to_node[lo + q];
+      int d = 0;
+      for_list(J, J->in_head, J->in_cnt, node, [&](int pred, int) {
+        const int r = J->rank[pred];
+        if (r >= lo && r <= hi) ++d;
+      });
+      deg[q] = d;
+    }
+    __syncwarp();
+    int done = 0;
+    if (lane == 0) {
+      int sp = 0;
+      for (int q = w - 1; q >= 0; --q)
+        if (deg[q] == 0) stack[sp++] = q;
+      while (sp > 0) {
+        const int q = stack[--sp];
+        const int node = J->rank_to_node[lo + q];
+        order[done++] = node;
+        for_list(J, J->out_head, J->out_cnt, node, [&](int succ, int) {
+          const int r = J->rank[succ];
+          if (r >= lo && r <= hi && --deg[r - lo] == 0) stack[sp++] = r - lo;
+        });
+      }
+    }
+    done = __shfl_sync(FULL, done, 0);
+    __syncwarp();
+    if (done != w) {
+      ok = false;
+      break;
+    }
+    for (int q = lane; q < w; q += 32) {
+      const int node = order[q];
+      J->rank[node] = lo + q;
+      J->rank_to_node[lo + q] = node;
+    }
+    __syncwarp();
+  }
+  return ok;
+}
+
 // Splices a read's new nodes into the current topological order (warp-wide):
 // each run of consecutive new nodes on the path is placed right after the
-// pre-existing path node before it. The result is a valid topological order
-// when consecutive pre-existing path nodes keep increasing ranks; otherwise
-// nothing is changed and false is returned (the caller then runs the LIFO
-// toposort of graph.rs:125-178). With a static band and no seeding the rank
-// order does not change any alignment: band guides, DP states and traceback
-// choices depend only on the predecessor / successor lists in insertion order.
+// pre-existing path node before it. Where two consecutive pre-existing path
+// nodes are out of order (the path reached an existing column sibling placed
+// after the node that follows it), the ranks between them, with the new nodes
+// spliced there, form a window; overlapping windows are merged and each is
+// re-sorted on its own by Kahn's algorithm over the edges inside it. Nodes
+// outside the windows keep their relative order and every edge into or out of
+// a window already points forward, so the result is a topological order. When
+// a window holds a cycle (or scratch is short) nothing usable is produced and
+// false is returned; the caller then runs the LIFO toposort of
+// graph.rs:125-178, which reports the cycle. With a static band and no
+// seeding the rank order does not change any alignment: band guides, DP
+// states and traceback choices depend only on the predecessor / successor
+// lists in insertion order.
 __device__ inline bool reorder_incremental(Job *J, const int4 *items, int n_items, int n_old, char *buf,
                                            int64_t buf_bytes) {
   const int lane = threadIdx.x & 31;
   const int n_new = J->n_nodes;
   if (J->n_rank != n_old || n_items <= 0) return false;
-  if (int64_t(4) * (2 * int64_t(n_old) + n_new) > buf_bytes) return false;
+  if (int64_t(4) * (2 * int64_t(n_old) + 4 * int64_t(n_new)) + int64_t(16) * (n_items + 2) > buf_bytes)
+    return false;
   int32_t *add = reinterpret_cast<int32_t *>(buf);
   int32_t *first = add + n_old;
   int32_t *nr2n = first + n_old;
+  int32_t *wdeg = nr2n + n_new;  // window scratch: degree, stack, order
+  int32_t *wstack = wdeg + n_new;
+  int32_t *worder = wstack + n_new;
+  int4 *spans = reinterpret_cast<int4 *>(align_up(reinterpret_cast<int64_t>(worder + n_new), 16));
   for (int r = lane; r < n_old; r += 32) add[r] = 0;
   __syncwarp();
   long long carry = -1;  // last pre-existing path item as (index << 32 | rank)
-  bool bad = false;
+  int n_spans = 0;
   for (int t0 = 0; t0 < n_items; t0 += 32) {
     const int t = t0 + lane;
     const int id = t < n_items ? items[t].w : -1;
@@ -1657,18 +1823,24 @@ __device__ inline bool reorder_incremental(Job *J, const int4 *items, int n_item
     long long prev = __shfl_up_sync(FULL, inc, 1);
     if (lane == 0) prev = -1;
     prev = prev > carry ? prev : carry;
+    bool out_of_order = false;
+    int pt = 0, pr = 0;
     if (old && prev >= 0) {
-      const int pt = int(prev >> 32), pr = int(prev & 0xffffffffLL);
-      if (pr >= rk) bad = true;
+      pt = int(prev >> 32);
+      pr = int(prev & 0xffffffffLL);
+      out_of_order = pr >= rk;
       if (t - pt - 1 > 0) {
         add[pr] = t - pt - 1;
         first[pr] = items[pt + 1].w;
       }
     }
+    const unsigned om = __ballot_sync(FULL, out_of_order);
+    if (out_of_order) spans[n_spans + __popc(om & ((1u << lane) - 1u))] = make_int4(items[pt].w, id, pr, 0);
+    n_spans += __popc(om);
     const long long last = __shfl_sync(FULL, inc, 31);
     carry = last > carry ? last : carry;
   }
-  if (__any_sync(FULL, bad) || carry < 0) return false;
+  if (carry < 0) return false;
   if (lane == 0) {
     const int pt = int(carry >> 32), pr = int(carry & 0xffffffffLL);
     if (n_items - pt - 1 > 0) {
@@ -1729,6 +1901,8 @@ __device__ inline bool reorder_incremental(Job *J, const int4 *items, int n_item
       if (r < n_new) J->rank_to_node[r] = v[u];
     }
   }
+  __syncwarp();
+  if (n_spans > 0 && !repair_windows(J, spans, n_spans, add, wdeg, wstack, worder)) return false;
   if (lane == 0) J->n_rank = n_new;
   __syncwarp();
   return true;

@@ -295,3 +295,19 @@ def test_batch_arena_overflow_parks_and_finishes(mp, oracle):
     assert st.relaunches >= 1
     for s, reads in enumerate(sets):
         assert batch.graph(s).dump() == oracle.align_sequences(params, reads).dump(5)
+
+
+def test_deep_high_error_sets_match_oracle(mp, oracle):
+    # many reads at high error: the path often reaches existing column
+    # siblings out of rank order, so the device repairs its rank order between
+    # reads; the finished graphs, ranks included, must be the oracle's
+    params = Params()
+    rng = np.random.default_rng(4242)
+    sets = [rc.synthetic_reads(rng, int(rng.integers(300, 700)), int(rng.integers(25, 40)), 0.09, 0.03, 0.03)
+            for _ in range(6)]
+    batch = mp.Batch(params, sets)
+    batch.run(0)
+    for s, reads in enumerate(sets):
+        assert batch.status(s) is None
+        o = oracle.align_sequences(params, reads, kernel=oracle.AUTO_AVX2)
+        assert batch.graph(s).dump() == o.dump(5)
