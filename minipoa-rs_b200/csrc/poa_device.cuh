@@ -98,6 +98,7 @@ struct Job {
   // outcome
   int32_t status, err_i, err_j, n_items;
   int32_t order_exact;  // 1 when rank is the reference's LIFO toposort order
+  int32_t giant;        // batched runs: a job far above the average size (gets its SM to itself)
   uint64_t cells;       // DP cells of completed reads (retries included)
   uint64_t dp_bytes;    // DP state bytes stored for those cells (M, D, I)
 };
@@ -1121,10 +1122,10 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
         Mx[g][1] = maxs(Mx[g][1], m4[g].x);
         Mx[g][2] = maxs(Mx[g][2], m4[g].y);
         Mx[g][3] = maxs(Mx[g][3], m4[g].z);
-        Dx[g][0] = maxs(Dx[g][0], maxs(d4[g].x + E, m4[g].x + O));
-        Dx[g][1] = maxs(Dx[g][1], maxs(d4[g].y + E, m4[g].y + O));
-        Dx[g][2] = maxs(Dx[g][2], maxs(d4[g].z + E, m4[g].z + O));
-        Dx[g][3] = maxs(Dx[g][3], maxs(d4[g].w + E, m4[g].w + O));
+        Dx[g][0] = __viaddmax_s32(d4[g].x, E, __viaddmax_s32(m4[g].x, O, Dx[g][0]));
+        Dx[g][1] = __viaddmax_s32(d4[g].y, E, __viaddmax_s32(m4[g].y, O, Dx[g][1]));
+        Dx[g][2] = __viaddmax_s32(d4[g].z, E, __viaddmax_s32(m4[g].z, O, Dx[g][2]));
+        Dx[g][3] = __viaddmax_s32(d4[g].w, E, __viaddmax_s32(m4[g].w, O, Dx[g][3]));
       }
     }
   }
@@ -1142,19 +1143,17 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int32_t prof = mrow[(bw >> (8 * k)) & 0xff];
-      Mx[g][k] = maxs(Mx[g][k] + prof, Dx[g][k]);  // Mx now holds md
-      X[g][k] = Mx[g][k] + O;
-      if (k > 0) X[g][k] = maxs(X[g][k], X[g][k - 1] + E);
+      Mx[g][k] = __viaddmax_s32(Mx[g][k], prof, Dx[g][k]);  // Mx now holds md
+      X[g][k] = k == 0 ? Mx[g][k] + O : __viaddmax_s32(X[g][k - 1], E, Mx[g][k] + O);
     }
   }
+  // (lanes below the shuffle distance get their own value back, and
+  // y + d*4E <= y because gap penalties are never positive)
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     int32_t y = X[g][3];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int32_t v = __shfl_up_sync(FULL, y, d);
-      if (lane >= d) y = maxs(y, v + d * 4 * E);
-    }
+    for (int d = 1; d < 32; d <<= 1) y = __viaddmax_s32(__shfl_up_sync(FULL, y, d), d * 4 * E, y);
     pre[g] = __shfl_up_sync(FULL, y, 1);
     if (lane == 0) pre[g] = BELOW;
   }
@@ -1164,8 +1163,8 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
   int32_t carry = NEG32;
 #pragma unroll
   for (int g = 0; g < G; ++g) {
-    cin[g] = maxs(pre[g], carry + 4 * lane * E);
-    if (g + 1 < G) carry = __shfl_sync(FULL, maxs(cin[g] + 4 * E, X[g][3]), 31);
+    cin[g] = __viaddmax_s32(carry, 4 * lane * E, pre[g]);
+    if (g + 1 < G) carry = __shfl_sync(FULL, __viaddmax_s32(cin[g], 4 * E, X[g][3]), 31);
   }
   __syncwarp();  // every predecessor read of the ring precedes this row's writes
 #pragma unroll
@@ -1174,7 +1173,7 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
     int32_t iv[4], mv[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      iv[k] = k == 0 ? cin[g] : maxs(X[g][k - 1], cin[g] + k * E);
+      iv[k] = k == 0 ? cin[g] : __viaddmax_s32(cin[g], k * E, X[g][k - 1]);
       mv[k] = maxs(Mx[g][k], iv[k]);
     }
     if (j0 < stop) {

@@ -1007,8 +1007,15 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
         sum += double(lens[r]);
       }
       const double w = 2.0 * (double(hp.b) + (hp.f ? mx / double(hp.f) : mx)) + 16.0;
-      est[size_t(s)] = sum * std::min(w, mx + 16.0);
+      // rows grow with the reads already fused into the graph
+      const double reads = double(set_off[s + 1] - set_off[s]);
+      est[size_t(s)] = sum * std::min(w, mx + 16.0) * (1.0 + 0.03 * reads);
     }
+    // giant jobs: well above the per-warp share of the whole batch
+    const double share = std::accumulate(est.begin(), est.end(), 0.0) /
+                         double(std::max(1, ctx->sm_count * batch_resident_warps_per_sm()));
+    for (int64_t s = 0; s < n_sets; ++s) b->jobs[size_t(s)].giant = est[size_t(s)] > 1.5 * share ? 1 : 0;
+    b->upload_jobs();
     b->order.resize(size_t(n_sets));
     std::iota(b->order.begin(), b->order.end(), 0);
     std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return est[a] > est[c]; });

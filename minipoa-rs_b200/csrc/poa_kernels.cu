@@ -25,46 +25,72 @@ __device__ __forceinline__ WarpSmem *warp_smem() {
 // largest jobs land on different SMs: the k-th warp to start on an SM takes
 // one of the positions [k * num_sms, (k + 1) * num_sms), in the order the SMs
 // reach that level; every later job comes from the shared queue, and a claim
-// flag per position makes each job run exactly once.
+// flag per position makes each job run exactly once. A giant job (marked by
+// the host, far above the average share) gets its SM to itself as far as the
+// schedule allows: the other warps of its block leave before taking a job,
+// and the SM's other warps take no new job while it runs. Their positions
+// and share of the queue go to the other SMs.
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *sched, int num_sms, DevParams P, char *arenas,
             int64_t slot_bytes, int slots) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  // the grid is rounded up to whole blocks; warps past the last slot own no arena
-  if (warp >= slots) return;
+  // the grid is rounded up to whole blocks; warps past the last slot own no
+  // arena (they leave after the block's start-up barrier)
+  const bool active = warp < slots;
   char *arena = arenas + warp * slot_bytes;
   WarpSmem *sm = warp_smem();
   int32_t *queue = sched;
   int32_t *sm_count = sched + 4;
   int32_t *level_count = sm_count + SCHED_SM_SLOTS;
-  int32_t *claim = level_count + SCHED_LEVELS;
-  int first = -1;
-  if (lane == 0) {
-    unsigned smid;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-    if (smid < unsigned(SCHED_SM_SLOTS)) {
-      const int level = atomicAdd(&sm_count[smid], 1);
-      if (level < SCHED_LEVELS) {
-        const int64_t p0 = int64_t(level) * num_sms + atomicAdd(&level_count[level], 1);
-        if (p0 < n_jobs && atomicExch(&claim[p0], 1) == 0) first = int(p0);
+  int32_t *sm_giant = level_count + SCHED_LEVELS;
+  int32_t *claim = sm_giant + SCHED_SM_SLOTS;
+  unsigned smid = 0;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  const bool sm_ok = smid < unsigned(SCHED_SM_SLOTS);
+  __shared__ int block_giant;
+  if (threadIdx.x == 0) block_giant = 0;
+  __syncthreads();
+  int first = -1, first_giant = 0;
+  if (active && lane == 0 && sm_ok) {
+    const int level = atomicAdd(&sm_count[smid], 1);
+    if (level < SCHED_LEVELS) {
+      const int64_t p0 = int64_t(level) * num_sms + atomicAdd(&level_count[level], 1);
+      if (p0 < n_jobs) {
+        first = int(p0);
+        first_giant = jobs[order[p0]].giant;
+        if (first_giant) atomicOr(&block_giant, 1);
       }
     }
   }
+  __syncthreads();
+  if (!active) return;
+  first = __shfl_sync(FULL, first, 0);
+  first_giant = __shfl_sync(FULL, first_giant, 0);
+  // the other warps of a giant's block leave its SM share to it; the queue
+  // positions they would have started with go to the shared queue
+  if (block_giant && !first_giant) return;
+  if (lane == 0 && first >= 0 && atomicExch(&claim[first], 1) != 0) first = -1;
   first = __shfl_sync(FULL, first, 0);
   for (;;) {
     int q = first;
     first = -1;
     if (q < 0) {
       if (lane == 0) {
-        do {
-          q = atomicAdd(queue, 1);
-        } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
+        if (sm_ok && atomicAdd(&sm_giant[smid], 0) != 0) {
+          q = n_jobs;  // this SM is running a giant job
+        } else {
+          do {
+            q = atomicAdd(queue, 1);
+          } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
+        }
       }
       q = __shfl_sync(FULL, q, 0);
       if (q >= n_jobs) break;
     }
     Job *J = jobs + order[q];
+    const bool giant = J->giant != 0 && sm_ok;
+    if (giant && lane == 0) atomicExch(&sm_giant[smid], 1);
     const int n_reads = J->n_reads;
     int32_t st = ST_OK;
     for (int r = J->next_read; r < n_reads; ++r) {
@@ -79,6 +105,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
         if (st == ST_OK) st = fs;
       }
       J->status = st;
+      if (giant) atomicExch(&sm_giant[smid], 0);
     }
     __syncwarp();
   }
