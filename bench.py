@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--sets", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=1003)
+    ap.add_argument("--lmax", type=int, default=5000, help="largest ancestor length (smaller for profiling runs)")
+    ap.add_argument("--dmax", type=int, default=60, help="largest read depth (smaller for profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-sets", type=int, default=64, help="sets timed in the plain per-read form")
@@ -197,7 +199,7 @@ def main():
     from minipoa_b200.params import Params
 
     params = Params()
-    sets = workloads.batched_sets(args.sets, seed=args.seed + rank)
+    sets = workloads.batched_sets(args.sets, seed=args.seed + rank, lmax=args.lmax, dmax=args.dmax)
 
     if args.impl == "reference":
         if rank != 0:
@@ -304,7 +306,8 @@ def main():
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "sets": args.sets, "seed": args.seed, "reads_per_step": reads // args.steps,
+            "config": {"workload": WORKLOAD.replace("200-5000", f"200-{args.lmax}").replace("10-60", f"10-{args.dmax}"),
+                       "sets": args.sets, "seed": args.seed, "reads_per_step": reads // args.steps,
                        "cells_per_step": cells // args.steps, "l2": "inputs larger than L2 (no flush needed)",
                        "parallelism": f"{world} independent GPU(s)", "slots": first_slots,
                        "relaunch_passes": first_passes, "reads_per_s": reads / (dev_ms / 1e3)},
