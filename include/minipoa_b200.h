@@ -12,7 +12,8 @@
  * own; a Rust FFI crate binds these declarations in an extern "C" block.
  *
  * Conventions: every call returns int status (POA_OK = 0); on failure
- * poa_last_error(ctx) gives the reference's error text. Buffers passed in are
+ * poa_last_error(ctx) gives the reference's error text (the calling thread's
+ * last error, so several threads can share a context's server). Buffers passed in are
  * caller-owned; buffers returned through out-pointers are library-owned and
  * released with poa_free. No call takes torch or other framework types.
  */
@@ -219,6 +220,69 @@ void poa_batch_free(poa_batch *batch);
 /* Tuning: concurrent warp slots per SM for the batched kernel (0 = auto) and
  * the DP arena bytes per slot (0 = auto from the budget). */
 int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot);
+
+/* ---- serving loop (no reference counterpart: the reference is a CLI that
+ * runs one job per process). Continuous batching: jobs (each one
+ * extend_graph over its reads, src/lib.rs:184-204, on a new graph) are
+ * submitted at any time; a dispatcher thread admits them in arrival order
+ * while the server's device pool holds their graph storage, reads and DP
+ * arena, and launches each admission round as one wave of the batched kernel
+ * on its own stream, so waves overlap on the device. A job's completion is
+ * seen as soon as its own warp finishes (host-mapped flag), not when its
+ * wave ends. A job whose DP outgrows its arena parks at its current read and
+ * is re-admitted with twice the arena. Finished graphs stay resident until
+ * released. Results are byte-identical to poa_align_sequences on the same
+ * reads, whatever else runs alongside. */
+typedef struct poa_server poa_server;
+enum {
+  POA_SERVER_QUEUED = 0,   /* waiting for admission */
+  POA_SERVER_RUNNING = 1,  /* on the device */
+  POA_SERVER_DONE = 2,     /* finished; output available until released */
+  POA_SERVER_FAILED = 3,   /* finished with an error (poa_server_job_info gives it) */
+  POA_SERVER_PARKED = 4    /* needs a larger DP arena; re-admitted when its wave ends */
+};
+typedef struct poa_server_job {
+  int32_t state;
+  int32_t reserved;
+  uint64_t cells;      /* band cells computed for the job */
+  double queued_ms;    /* submission to first launch */
+  double latency_ms;   /* submission to completion (0 while unfinished) */
+} poa_server_job;
+typedef struct poa_server_stats {
+  uint64_t done_jobs;
+  uint64_t done_cells;
+  uint64_t waves;          /* kernel launches so far */
+  uint64_t queued;         /* jobs waiting for admission */
+  uint64_t running_waves;
+  uint64_t pool_bytes;
+  uint64_t pool_used;
+  double busy_s;           /* first submission to the last completion */
+} poa_server_stats;
+/* pool_bytes: device memory of the server (0 = what the context's budget
+ * leaves, less 512 MiB); streams: concurrent waves (0 = 64). */
+int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_bytes, int32_t streams,
+                      poa_server **out);
+/* Queues one job (its reads in order); returns at once with its id. */
+int poa_server_submit(poa_ctx *ctx, poa_server *server, int64_t n_seqs, const uint8_t *const *seqs,
+                      const int64_t *lens, int64_t *job_id);
+/* Waits for a job to finish (timeout_ms < 0: no limit; POA_ERR_TIMEOUT when
+ * it runs out). */
+int poa_server_wait(poa_ctx *ctx, poa_server *server, int64_t job, double timeout_ms, int32_t *state);
+/* State and timings of a job; a failed job returns its error. */
+int poa_server_job_info(poa_ctx *ctx, poa_server *server, int64_t job, poa_server_job *out);
+/* Output of a finished job: result 0 consensus FASTA, 1 MSA, 2 GFA (names
+ * "read{i}" and empty comments unless given). */
+int poa_server_output(poa_ctx *ctx, poa_server *server, int64_t job, int32_t result, const char *const *names,
+                      const char *const *comments, char **out, int64_t *out_len);
+/* Frees a finished job's graph. */
+int poa_server_release(poa_ctx *ctx, poa_server *server, int64_t job);
+/* Scales the DP arena a job is first admitted with (default 1: an estimate
+ * of its widest band over the rows its graph grows to). Below 1 a job takes
+ * less memory and parks more often; for memory-tight deployments. */
+int poa_server_tune(poa_ctx *ctx, poa_server *server, double arena_scale);
+int poa_server_stats_get(poa_ctx *ctx, poa_server *server, poa_server_stats *out);
+/* Finishes the queued and running jobs, then frees the server. */
+void poa_server_destroy(poa_server *server);
 
 #ifdef __cplusplus
 }

@@ -99,6 +99,9 @@ struct Job {
   int32_t status, err_i, err_j, n_items;
   int32_t order_exact;  // 1 when rank is the reference's LIFO toposort order
   int32_t giant;        // batched runs: a job far above the average size (gets its SM to itself)
+  char *arena;          // when set, the job's own DP arena (serving); else the warp slot's
+  int64_t arena_bytes;
+  int32_t *done_flag;   // when set (host-mapped memory), raised once the job leaves the kernel
   uint64_t cells;       // DP cells of completed reads (retries included)
   uint64_t dp_bytes;    // DP state bytes stored for those cells (M, D, I)
 };

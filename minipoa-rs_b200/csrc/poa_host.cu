@@ -3,10 +3,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -136,6 +141,9 @@ std::vector<uint8_t> encode_table(const HostParams &p) {
 }
 
 thread_local std::string g_create_error;
+// The message of the calling thread's last failed call: the server API is
+// called from several threads at once (submit on one, wait on others).
+thread_local std::string t_last_error;
 
 char *dup_string(const std::string &s) {
   char *o = (char *)std::malloc(s.size() + 1);
@@ -154,7 +162,6 @@ struct poa_ctx {
   cudaStream_t stream = nullptr;
   uint64_t budget = 0;
   uint64_t allocated = 0;
-  std::string err;
   char *arena = nullptr;
   int64_t arena_bytes = 0;
   uint8_t *qbuf = nullptr;
@@ -386,18 +393,19 @@ poa_graph *new_graph(poa_ctx *ctx, const HostParams &hp, Caps caps) {
 
 template <class F>
 int api(poa_ctx *ctx, F &&f) {
+  (void)ctx;
   try {
     f();
-    if (ctx) ctx->err.clear();
+    t_last_error.clear();
     return POA_OK;
   } catch (const AlignError &e) {
-    if (ctx) ctx->err = e.msg;
+    t_last_error = e.msg;
     return e.code;
   } catch (const CudaError &e) {
-    if (ctx) ctx->err = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    t_last_error = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
     return POA_ERR_CUDA;
   } catch (const std::bad_alloc &) {
-    if (ctx) ctx->err = "host allocation failed";
+    t_last_error = "host allocation failed";
     return POA_ERR_ALLOC;
   }
 }
@@ -655,7 +663,7 @@ int poa_ctx_create(int device, uint64_t mem_budget, poa_ctx **out) {
     ctx->budget = mem_budget ? std::min<uint64_t>(mem_budget, free_b) : uint64_t(double(free_b) * 0.9);
   });
   if (rc != POA_OK) {
-    g_create_error = ctx->err;
+    g_create_error = t_last_error;
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     return rc;
   }
@@ -675,8 +683,9 @@ void poa_ctx_destroy(poa_ctx *ctx) {
   delete ctx;
 }
 
-// With a null context: the error of the last failed poa_ctx_create.
-const char *poa_last_error(const poa_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+// The calling thread's last error; with a null context, that of its last
+// failed poa_ctx_create.
+const char *poa_last_error(const poa_ctx *ctx) { return ctx ? t_last_error.c_str() : g_create_error.c_str(); }
 void poa_free(void *ptr) { std::free(ptr); }
 
 int poa_params_validate(poa_ctx *ctx, const poa_params *params) {
@@ -1260,6 +1269,623 @@ void poa_batch_free(poa_batch *batch) { delete batch; }
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Serving loop: continuous batching of independent jobs (read sets, optionally
+// extending a graph built from earlier reads). Jobs are admitted in arrival
+// order while the server's device pool holds their graph storage, reads and
+// DP arena; every admission round launches the admitted jobs as one wave of
+// the batched kernel on its own stream, so waves that arrive while others run
+// overlap on the device. Finished graphs stay resident until released.
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// First-fit allocator over one device pool, in 256-byte granules.
+struct PoolAlloc {
+  char *base = nullptr;
+  uint64_t size = 0, used = 0;
+  std::map<uint64_t, uint64_t> free_;  // offset -> bytes
+  void init(char *b, uint64_t n) {
+    base = b;
+    size = n;
+    used = 0;
+    free_.clear();
+    if (n) free_[0] = n;
+  }
+  static uint64_t round(uint64_t n) { return (n + 255) / 256 * 256; }
+  char *take(uint64_t bytes) {
+    bytes = round(std::max<uint64_t>(bytes, 1));
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const uint64_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > bytes) free_[off + bytes] = len - bytes;
+      used += bytes;
+      return base + off;
+    }
+    return nullptr;
+  }
+  void give(char *p, uint64_t bytes) {
+    if (!p) return;
+    bytes = round(std::max<uint64_t>(bytes, 1));
+    used -= std::min(used, bytes);
+    auto it = free_.emplace(uint64_t(p - base), bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct ServerJob {
+  int64_t id = 0;
+  std::vector<uint8_t> bytes;  // the reads, back to back
+  std::vector<int64_t> lens;
+  Caps caps;
+  uint64_t storage_bytes = 0, reads_bytes = 0, arena_bytes = 0;
+  char *storage = nullptr, *reads = nullptr, *arena = nullptr;
+  Job J{};  // host copy of the device descriptor
+  Job *d_desc = nullptr;  // its device copy while a wave runs it
+  int done_slot = -1;     // host-mapped flag the kernel raises when the job leaves it
+  bool fresh = true;
+  int32_t state = POA_SERVER_QUEUED;
+  std::string error;
+  double t_submit = 0, t_start = 0, t_done = 0;
+};
+
+struct Wave {
+  int stream = 0;
+  cudaEvent_t done = nullptr;
+  std::vector<int64_t> ids;
+  char *mem = nullptr;
+  uint64_t mem_bytes = 0;
+  Job *d_jobs = nullptr;
+};
+
+}  // namespace
+
+struct poa_server {
+  poa_ctx *ctx = nullptr;
+  HostParams hp;
+  DevParams P{};
+  char *pool_mem = nullptr;
+  uint64_t pool_bytes = 0;
+  PoolAlloc pool;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::map<int64_t, std::unique_ptr<ServerJob>> jobs;
+  std::deque<int64_t> pending;
+  std::vector<Wave> waves;
+  std::vector<cudaStream_t> streams;
+  std::vector<int> free_streams;
+  cudaStream_t out_stream = nullptr;
+  std::thread worker;
+  bool stop = false;
+  int64_t next_id = 0;
+  int32_t *h_done = nullptr;  // host-mapped completion flags
+  int32_t *d_done = nullptr;
+  std::vector<int> free_done;
+  std::vector<int64_t> running;  // jobs on the device
+  std::string fatal;
+  double arena_scale = 1.0;  // multiplies the first DP arena of each job
+  // statistics of finished jobs
+  uint64_t done_jobs = 0, done_cells = 0, launched_waves = 0;
+  double first_submit = -1, last_done = 0;
+
+  ~poa_server() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv.notify_all();
+    if (worker.joinable()) worker.join();
+    for (auto &w : waves) {
+      cudaEventSynchronize(w.done);
+      cudaEventDestroy(w.done);
+    }
+    for (auto st : streams) cudaStreamDestroy(st);
+    if (out_stream) cudaStreamDestroy(out_stream);
+    if (h_done) cudaFreeHost(h_done);
+    if (ctx) ctx->dfree(pool_mem, pool_bytes);
+  }
+
+  // Bytes a job needs beyond its arena: graph storage and reads.
+  static void size_job(ServerJob &sj, int sigma) {
+    int64_t sum = 0;
+    const int64_t k = int64_t(sj.lens.size());
+    for (int64_t l : sj.lens) sum += l;
+    Caps c;
+    c.sigma = sigma;
+    c.node_cap = int32_t(std::min<int64_t>(sum + 2 * k + 8, INT32_MAX / 2));
+    c.chunk_cap = int32_t(std::min<int64_t>(2 * (sum + 3 * k) + 16, INT32_MAX / 2));
+    c.path_cap = int32_t(std::min<int64_t>(sum + k + 1, INT32_MAX / 2));
+    c.max_paths = int32_t(k + 1);
+    sj.caps = c;
+    Job J{};
+    sj.storage_bytes = layout(c, nullptr, &J) + 256;
+    sj.reads_bytes = uint64_t(k) * 12 + uint64_t(sum) + 64;
+  }
+  // First DP arena of a job: band cells of its widest read over an estimate of
+  // the rows the graph grows to, plus per-row scratch; a job that needs more
+  // parks and comes back with twice the arena.
+  uint64_t first_arena(const ServerJob &sj) const {
+    int64_t mx = 0;
+    for (int64_t l : sj.lens) mx = std::max(mx, l);
+    const double band = std::min(2.0 * (double(hp.b) + (hp.f ? double(mx) / double(hp.f) : double(mx))) + 16.0,
+                                 double(mx) + 16.0);
+    const double rows = double(mx) * (1.0 + 0.1 * double(sj.lens.size())) + 16.0;
+    return uint64_t(arena_scale * rows * (band * 12.0 + 400.0)) + (uint64_t(1) << 20);
+  }
+
+  void run();
+  void finish_wave(Wave &w);
+  bool finish_jobs();
+  bool launch_wave();
+};
+
+// Jobs whose completion flag is up: their descriptor is read back and their
+// arena and reads go back to the pool while the rest of the wave runs. Parked
+// jobs (arena too small) are requeued when their wave ends.
+bool poa_server::finish_jobs() {
+  std::vector<int64_t> ready;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (int64_t id : running) {
+      const ServerJob &sj = *jobs.at(id);
+      if (reinterpret_cast<volatile int32_t *>(h_done)[sj.done_slot] != 0) ready.push_back(id);
+    }
+  }
+  if (ready.empty()) return false;
+  for (int64_t id : ready) {
+    Job hj{};
+    Job *src = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      src = jobs.at(id)->d_desc;
+    }
+    CK(cudaMemcpyAsync(&hj, src, sizeof(Job), cudaMemcpyDeviceToHost, out_stream));
+    CK(cudaStreamSynchronize(out_stream));
+    const double t = now_s();
+    std::lock_guard<std::mutex> lk(mu);
+    ServerJob &sj = *jobs.at(id);
+    running.erase(std::find(running.begin(), running.end(), id));
+    free_done.push_back(sj.done_slot);
+    sj.done_slot = -1;
+    sj.J = hj;
+    if (hj.status == ST_ARENA_FULL) {
+      sj.state = POA_SERVER_PARKED;
+      continue;
+    }
+    pool.give(sj.arena, sj.arena_bytes);
+    pool.give(sj.reads, sj.reads_bytes);
+    sj.arena = sj.reads = nullptr;
+    sj.t_done = t;
+    if (hj.status == ST_OK) {
+      sj.state = POA_SERVER_DONE;
+      done_cells += hj.cells;
+    } else {
+      sj.state = POA_SERVER_FAILED;
+      sj.error = status_message(hj.status, hj.err_i, hj.err_j);
+    }
+    ++done_jobs;
+    last_done = t;
+  }
+  cv.notify_all();
+  return true;
+}
+
+void poa_server::finish_wave(Wave &w) {
+  finish_jobs();  // flags raised just before the wave ended
+  std::lock_guard<std::mutex> lk(mu);
+  for (int64_t id : w.ids) {
+    ServerJob &sj = *jobs.at(id);
+    sj.d_desc = nullptr;
+    if (sj.state != POA_SERVER_PARKED) continue;
+    // the graph is intact at its next read; come back with twice the arena
+    pool.give(sj.arena, sj.arena_bytes);
+    sj.arena = nullptr;
+    sj.arena_bytes *= 2;
+    sj.J.status = ST_OK;
+    sj.fresh = false;
+    sj.state = POA_SERVER_QUEUED;
+    pending.push_front(sj.id);
+  }
+  pool.give(w.mem, w.mem_bytes);
+  free_streams.push_back(w.stream);
+  cudaEventDestroy(w.done);
+  cv.notify_all();
+}
+
+// Admits queued jobs in arrival order while the pool holds them and launches
+// them as one wave; returns whether a wave was launched.
+bool poa_server::launch_wave() {
+  Wave w;
+  std::vector<ServerJob *> adm;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (pending.empty() || free_streams.empty()) return false;
+    while (!pending.empty() && adm.size() < free_done.size()) {
+      ServerJob &sj = *jobs.at(pending.front());
+      char *st = sj.storage ? sj.storage : pool.take(sj.storage_bytes);
+      char *rd = sj.reads ? sj.reads : (st ? pool.take(sj.reads_bytes) : nullptr);
+      char *ar = (st && rd) ? pool.take(sj.arena_bytes) : nullptr;
+      if (!ar) {
+        if (!sj.storage) pool.give(st, sj.storage_bytes);
+        if (!sj.reads) pool.give(rd, sj.reads_bytes);
+        // a job larger than the whole idle pool can never run
+        if (waves.empty() && adm.empty()) {
+          pool.give(sj.reads, sj.reads_bytes);
+          sj.reads = nullptr;
+          sj.state = POA_SERVER_FAILED;
+          sj.error = "job needs more device memory than the server pool";
+          sj.t_done = now_s();
+          pending.pop_front();
+          cv.notify_all();
+          continue;
+        }
+        break;
+      }
+      sj.storage = st;
+      sj.reads = rd;
+      sj.arena = ar;
+      pending.pop_front();
+      adm.push_back(&sj);
+    }
+    if (adm.empty()) return false;
+    w.mem_bytes = adm.size() * sizeof(Job) + sched_words(adm.size()) * 4 + adm.size() * 4 + 1024;
+    w.mem = pool.take(w.mem_bytes);
+    if (!w.mem) {
+      for (auto it = adm.rbegin(); it != adm.rend(); ++it) {
+        pool.give((*it)->arena, (*it)->arena_bytes);
+        (*it)->arena = nullptr;
+        pending.push_front((*it)->id);
+      }
+      return false;
+    }
+    w.stream = free_streams.back();
+    free_streams.pop_back();
+  }
+  // fresh jobs first (they are reset to Graph::new), parked ones keep their graph
+  std::stable_partition(adm.begin(), adm.end(), [](const ServerJob *j) { return j->fresh; });
+  const cudaStream_t stream = streams[size_t(w.stream)];
+  const double t = now_s();
+  std::vector<Job> hj(adm.size());
+  int n_fresh = 0;
+  for (size_t k = 0; k < adm.size(); ++k) {
+    ServerJob &sj = *adm[k];
+    if (sj.fresh) {
+      ++n_fresh;
+      Job J{};
+      layout(sj.caps, sj.storage, &J);
+      const int64_t n = int64_t(sj.lens.size());
+      J.read_off = reinterpret_cast<int64_t *>(sj.reads);
+      J.read_len = reinterpret_cast<int32_t *>(sj.reads + n * 8);
+      J.reads = reinterpret_cast<uint8_t *>(sj.reads + n * 12);
+      J.n_reads = int32_t(n);
+      std::vector<char> host(sj.reads_bytes, 0);
+      int64_t at = 0;
+      for (int64_t r = 0; r < n; ++r) {
+        reinterpret_cast<int64_t *>(host.data())[r] = at;
+        reinterpret_cast<int32_t *>(host.data() + n * 8)[r] = int32_t(sj.lens[size_t(r)]);
+        at += sj.lens[size_t(r)];
+      }
+      if (!sj.bytes.empty()) std::memcpy(host.data() + n * 12, sj.bytes.data(), sj.bytes.size());
+      CK(cudaMemcpyAsync(sj.reads, host.data(), sj.reads_bytes, cudaMemcpyHostToDevice, stream));
+      CK(cudaStreamSynchronize(stream));  // the staging vector goes out of scope
+      sj.J = J;
+      sj.t_start = t;
+    }
+    sj.J.arena = sj.arena;
+    sj.J.arena_bytes = int64_t(sj.arena_bytes);
+    sj.J.giant = 0;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      sj.done_slot = free_done.back();
+      free_done.pop_back();
+    }
+    h_done[sj.done_slot] = 0;
+    sj.J.done_flag = d_done + sj.done_slot;
+    sj.state = POA_SERVER_RUNNING;
+    hj[k] = sj.J;
+    w.ids.push_back(sj.id);
+  }
+  char *m = w.mem;
+  w.d_jobs = reinterpret_cast<Job *>(m);
+  int32_t *d_order = reinterpret_cast<int32_t *>(m + PoolAlloc::round(hj.size() * sizeof(Job)));
+  int32_t *d_sched = d_order + (hj.size() + 63) / 64 * 64;
+  std::vector<int32_t> order(hj.size());
+  std::iota(order.begin(), order.end(), 0);
+  CK(cudaMemcpyAsync(w.d_jobs, hj.data(), hj.size() * sizeof(Job), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemsetAsync(d_sched, 0, sched_words(hj.size()) * 4, stream));
+  if (n_fresh) CK(launch_reset(w.d_jobs, n_fresh, P.sigma, P.unknown, stream));
+  CK(launch_batch(w.d_jobs, d_order, int(hj.size()), d_sched, ctx->sm_count, P, nullptr, 0, int(hj.size()), stream));
+  CK(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
+  CK(cudaEventRecord(w.done, stream));
+  std::lock_guard<std::mutex> lk(mu);
+  for (size_t k = 0; k < adm.size(); ++k) {
+    adm[k]->d_desc = w.d_jobs + k;
+    running.push_back(adm[k]->id);
+  }
+  ++launched_waves;
+  waves.push_back(w);
+  return true;
+}
+
+void poa_server::run() {
+  cudaSetDevice(ctx->device);
+  try {
+    for (;;) {
+      bool progress = false;
+      // finished waves
+      for (size_t k = 0; k < waves.size();) {
+        const cudaError_t e = cudaEventQuery(waves[k].done);
+        if (e == cudaErrorNotReady) {
+          ++k;
+          continue;
+        }
+        CK(e);
+        Wave w = waves[k];
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          waves.erase(waves.begin() + long(k));
+        }
+        finish_wave(w);
+        progress = true;
+      }
+      if (finish_jobs()) progress = true;
+      if (launch_wave()) progress = true;
+      std::unique_lock<std::mutex> lk(mu);
+      if (stop && pending.empty() && waves.empty()) break;
+      if (!progress) cv.wait_for(lk, std::chrono::microseconds(waves.empty() ? 2000 : 50));
+    }
+  } catch (const CudaError &e) {
+    std::lock_guard<std::mutex> lk(mu);
+    fatal = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
+    for (auto &kv : jobs)
+      if (kv.second->state == POA_SERVER_QUEUED || kv.second->state == POA_SERVER_RUNNING) {
+        kv.second->state = POA_SERVER_FAILED;
+        kv.second->error = fatal;
+      }
+    pending.clear();
+    cv.notify_all();
+  }
+}
+
+extern "C" {
+
+int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_bytes, int32_t streams,
+                      poa_server **out) {
+  if (out) *out = nullptr;
+  if (!ctx || !out) return POA_ERR_INVALID;
+  std::unique_ptr<poa_server> sv(new poa_server());
+  const int rc = api(ctx, [&] {
+    sv->hp = checked_params(params);
+    if (sv->hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
+    if (sv->hp.progressive) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
+    if (streams <= 0) streams = 64;
+    const uint64_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
+    if (pool_bytes == 0) pool_bytes = left > (uint64_t(512) << 20) ? left - (uint64_t(512) << 20) : 0;
+    pool_bytes = pool_bytes / 256 * 256;  // the scoring tables follow the pool, 256-byte aligned
+    if (pool_bytes < (uint64_t(64) << 20)) throw AlignError{POA_ERR_ALLOC, "server pool below 64 MiB"};
+    const size_t mat = sv->hp.matrix.size() * 4 + 256 + 256;
+    sv->pool_mem = (char *)ctx->dalloc(pool_bytes + mat);
+    sv->ctx = ctx;
+    sv->pool_bytes = pool_bytes + mat;
+    int32_t *d_matrix = reinterpret_cast<int32_t *>(sv->pool_mem + pool_bytes);
+    uint8_t *d_encode = reinterpret_cast<uint8_t *>(sv->pool_mem + pool_bytes + (sv->hp.matrix.size() * 4 + 255) / 256 * 256);
+    CK(cudaMemcpy(d_matrix, sv->hp.matrix.data(), sv->hp.matrix.size() * 4, cudaMemcpyHostToDevice));
+    auto enc = encode_table(sv->hp);
+    CK(cudaMemcpy(d_encode, enc.data(), 256, cudaMemcpyHostToDevice));
+    sv->P = poa_ctx::make_params(sv->hp, d_matrix, d_encode);
+    sv->pool.init(sv->pool_mem, pool_bytes);
+    for (int k = 0; k < streams; ++k) {
+      cudaStream_t st = nullptr;
+      CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      sv->streams.push_back(st);
+      sv->free_streams.push_back(k);
+    }
+    CK(cudaStreamCreateWithFlags(&sv->out_stream, cudaStreamNonBlocking));
+    constexpr int kDoneSlots = 1 << 16;
+    CK(cudaHostAlloc(reinterpret_cast<void **>(&sv->h_done), kDoneSlots * 4, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&sv->d_done), sv->h_done, 0));
+    for (int k = kDoneSlots - 1; k >= 0; --k) sv->free_done.push_back(k);
+    poa_server *raw = sv.get();
+    sv->worker = std::thread([raw] { raw->run(); });
+  });
+  if (rc == POA_OK) *out = sv.release();
+  return rc;
+}
+
+void poa_server_destroy(poa_server *server) { delete server; }
+
+int poa_server_submit(poa_ctx *ctx, poa_server *sv, int64_t n_seqs, const uint8_t *const *seqs, const int64_t *lens,
+                      int64_t *job_id) {
+  if (!ctx || !sv || !job_id || (n_seqs > 0 && (!seqs || !lens)) || n_seqs < 0) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    auto sj = std::make_unique<ServerJob>();
+    int64_t total = 0;
+    for (int64_t r = 0; r < n_seqs; ++r) {
+      if (lens[r] < 0 || lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+      total += lens[r];
+    }
+    sj->bytes.resize(size_t(total));
+    sj->lens.assign(lens, lens + n_seqs);
+    int64_t at = 0;
+    for (int64_t r = 0; r < n_seqs; ++r) {
+      if (lens[r]) std::memcpy(sj->bytes.data() + at, seqs[r], size_t(lens[r]));
+      at += lens[r];
+    }
+    poa_server::size_job(*sj, int(sv->hp.alphabet.size()));
+    sj->arena_bytes = sv->first_arena(*sj);
+    sj->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!sv->fatal.empty()) throw AlignError{POA_ERR_CUDA, sv->fatal};
+    sj->id = sv->next_id++;
+    *job_id = sj->id;
+    if (sv->first_submit < 0) sv->first_submit = sj->t_submit;
+    sv->pending.push_back(sj->id);
+    sv->jobs[sj->id] = std::move(sj);
+    sv->cv.notify_all();
+  });
+}
+
+int poa_server_wait(poa_ctx *ctx, poa_server *sv, int64_t job, double timeout_ms, int32_t *state) {
+  if (!ctx || !sv) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(job);
+    if (it == sv->jobs.end()) throw AlignError{POA_ERR_INVALID, "unknown job"};
+    ServerJob &sj = *it->second;
+    auto finished = [&] { return sj.state == POA_SERVER_DONE || sj.state == POA_SERVER_FAILED; };
+    if (timeout_ms < 0)
+      sv->cv.wait(lk, finished);
+    else
+      sv->cv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), finished);
+    if (state) *state = sj.state;
+    if (!finished() && timeout_ms >= 0) throw AlignError{POA_ERR_TIMEOUT, "job not finished within the timeout"};
+  });
+}
+
+int poa_server_job_info(poa_ctx *ctx, poa_server *sv, int64_t job, poa_server_job *out) {
+  if (!ctx || !sv || !out) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(job);
+    if (it == sv->jobs.end()) throw AlignError{POA_ERR_INVALID, "unknown job"};
+    const ServerJob &sj = *it->second;
+    out->state = sj.state;
+    out->reserved = 0;
+    out->cells = sj.J.cells;
+    out->queued_ms = (sj.t_start > 0 ? sj.t_start - sj.t_submit : 0) * 1e3;
+    out->latency_ms = (sj.t_done > 0 ? sj.t_done - sj.t_submit : 0) * 1e3;
+    if (sj.state == POA_SERVER_FAILED) throw AlignError{POA_ERR_ALIGN, sj.error};
+  });
+}
+
+int poa_server_output(poa_ctx *ctx, poa_server *sv, int64_t job, int32_t result, const char *const *names,
+                      const char *const *comments, char **out, int64_t *out_len) {
+  if (out) *out = nullptr;
+  if (out_len) *out_len = 0;
+  if (!ctx || !sv || !out || !out_len) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    Job J{};
+    int64_t k = 0;
+    char *tmp = nullptr;
+    uint64_t tmp_bytes = 0, words = 0;
+    const int sigma = int(sv->hp.alphabet.size());
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      auto it = sv->jobs.find(job);
+      if (it == sv->jobs.end()) throw AlignError{POA_ERR_INVALID, "unknown job"};
+      ServerJob &sj = *it->second;
+      if (sj.state == POA_SERVER_FAILED) throw AlignError{POA_ERR_ALIGN, sj.error};
+      if (sj.state != POA_SERVER_DONE) throw AlignError{POA_ERR_INVALID, "job has not finished"};
+      J = sj.J;
+      k = int64_t(sj.lens.size());
+      words = uint64_t(packed_words(J, sigma));
+      tmp_bytes = 1024 + words * 4 + 16;
+      tmp = sv->pool.take(tmp_bytes);
+      if (!tmp) throw AlignError{POA_ERR_ALLOC, "server pool has no room for the output"};
+    }
+    std::vector<int32_t> rec(words + 1);
+    auto release = [&] {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->pool.give(tmp, tmp_bytes);
+    };
+    try {
+      Job *d_job = reinterpret_cast<Job *>(tmp);
+      int64_t *d_off = reinterpret_cast<int64_t *>(tmp + 512);
+      int32_t *d_id = reinterpret_cast<int32_t *>(tmp + 768);
+      int32_t *d_out = reinterpret_cast<int32_t *>(tmp + 1024);
+      const int64_t offs[2] = {0, int64_t(words)};
+      const int32_t id0 = 0;
+      cudaStream_t st = sv->out_stream;
+      CK(cudaMemcpyAsync(d_job, &J, sizeof(Job), cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(d_off, offs, sizeof(offs), cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(d_id, &id0, 4, cudaMemcpyHostToDevice, st));
+      CK(launch_pack(d_job, d_id, 1, d_off, d_out, sigma, st));
+      CK(cudaMemcpyAsync(rec.data(), d_out, words * 4, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+    HostGraph g = HostGraph::parse(rec.data());
+    auto nm = name_list(k, names, "read");
+    std::vector<std::string> cm(static_cast<size_t>(k));
+    for (int64_t i = 0; i < k && comments; ++i) cm[size_t(i)] = comments[i];
+    std::string s, err;
+    if (result == 0) {
+      std::vector<uint8_t> sq;
+      std::vector<int64_t> ids, cv;
+      g.consensus(sv->hp, sq, ids, cv);
+      s = ">consensus sequence\n" + std::string(sq.begin(), sq.end()) + "\n";
+    } else if (result == 1) {
+      if (!g.msa(sv->hp, nm, cm, s, err)) throw AlignError{POA_ERR_ALIGN, err};
+    } else if (result == 2) {
+      if (!g.gfa(sv->hp, nm, s, err)) throw AlignError{POA_ERR_ALIGN, err};
+    } else {
+      throw AlignError{POA_ERR_INVALID, "result format and verbosity must be 0..2"};
+    }
+    *out = dup_string(s);
+    *out_len = int64_t(s.size());
+  });
+}
+
+int poa_server_release(poa_ctx *ctx, poa_server *sv, int64_t job) {
+  if (!ctx || !sv) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(job);
+    if (it == sv->jobs.end()) throw AlignError{POA_ERR_INVALID, "unknown job"};
+    ServerJob &sj = *it->second;
+    if (sj.state != POA_SERVER_DONE && sj.state != POA_SERVER_FAILED)
+      throw AlignError{POA_ERR_INVALID, "job has not finished"};
+    sv->pool.give(sj.storage, sj.storage_bytes);
+    sv->jobs.erase(it);
+    sv->cv.notify_all();
+  });
+}
+
+int poa_server_tune(poa_ctx *ctx, poa_server *sv, double arena_scale) {
+  if (!ctx || !sv) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    if (!(arena_scale > 0.0) || arena_scale > 1e6) throw AlignError{POA_ERR_INVALID, "arena scale must be positive"};
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->arena_scale = arena_scale;
+  });
+}
+
+int poa_server_stats_get(poa_ctx *ctx, poa_server *sv, poa_server_stats *out) {
+  if (!ctx || !sv || !out) return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    out->done_jobs = sv->done_jobs;
+    out->done_cells = sv->done_cells;
+    out->waves = sv->launched_waves;
+    out->queued = uint64_t(sv->pending.size());
+    out->running_waves = uint64_t(sv->waves.size());
+    out->pool_bytes = sv->pool.size;
+    out->pool_used = sv->pool.used;
+    out->busy_s = sv->first_submit >= 0 ? sv->last_done - sv->first_submit : 0;
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Accessors for entry points defined in other translation units.
 namespace poa {
 
@@ -1267,7 +1893,10 @@ Job *graph_device_job(poa_graph *g) { return g->d_job; }
 int graph_alphabet(const poa_graph *g) { return g->sigma; }
 cudaStream_t ctx_stream(const poa_ctx *c) { return c->stream; }
 int ctx_device(const poa_ctx *c) { return c->device; }
-void ctx_set_error(poa_ctx *c, const std::string &msg) { c->err = msg; }
+void ctx_set_error(poa_ctx *c, const std::string &msg) {
+  (void)c;
+  t_last_error = msg;
+}
 std::string describe_status(int32_t st, int err_i, int err_j) { return status_message(st, err_i, err_j); }
 int status_to_code(int32_t st) { return status_code(st); }
 

@@ -92,20 +92,26 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     const bool giant = J->giant != 0 && sm_ok;
     if (giant && lane == 0) atomicExch(&sm_giant[smid], 1);
     const int n_reads = J->n_reads;
+    char *ja = J->arena ? J->arena : arena;
+    const int64_t jb = J->arena ? J->arena_bytes : slot_bytes;
     int32_t st = ST_OK;
     for (int r = J->next_read; r < n_reads; ++r) {
-      st = extend_one(J, P, arena, slot_bytes, J->reads + J->read_off[r], J->read_len[r], r, sm);
+      st = extend_one(J, P, ja, jb, J->reads + J->read_off[r], J->read_len[r], r, sm);
       if (st != ST_OK) break;
     }
     // a finished (or failed) job ends with the reference's exact rank order;
     // a parked job keeps its order for the next pass
     if (lane == 0) {
       if (st == ST_OK || is_alignment_error(st)) {
-        const int32_t fs = finalize_order(J, arena, slot_bytes);
+        const int32_t fs = finalize_order(J, ja, jb);
         if (st == ST_OK) st = fs;
       }
       J->status = st;
       if (giant) atomicExch(&sm_giant[smid], 0);
+      if (J->done_flag) {
+        __threadfence_system();  // the descriptor before the flag the host polls
+        *reinterpret_cast<volatile int32_t *>(J->done_flag) = 1;
+      }
     }
     __syncwarp();
   }

@@ -3,9 +3,10 @@
 Mirrors the reference library: Params, Sequence, AlignedBase (src/lib.rs),
 align_sequences / extend_graph / run / dp_backend (src/lib.rs), align / poa
 (src/align.rs) and Graph (src/graph.rs), over the C ABI of
-include/minipoa_b200.h. Batch runs many independent read sets on the GPU.
+include/minipoa_b200.h. Batch runs many independent read sets on the GPU;
+Server admits read sets as they arrive (continuous batching).
 """
 from .params import AlignedBase, CParams, Params, Sequence, default_matrix  # noqa: F401
 from .api import (  # noqa: F401
-    Batch, Context, Graph, PoaError, align, align_sequences, default_context, dp_backend, extend_graph, poa, run,
+    Batch, Context, Graph, PoaError, Server, align, align_sequences, default_context, dp_backend, extend_graph, poa, run,
 )

@@ -26,6 +26,20 @@ class GraphSizes(ctypes.Structure):
                 ("n_rank", ctypes.c_int64)]
 
 
+class ServerJobInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("reserved", ctypes.c_int32), ("cells", ctypes.c_uint64),
+                ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("done_jobs", ctypes.c_uint64), ("done_cells", ctypes.c_uint64), ("waves", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("running_waves", ctypes.c_uint64), ("pool_bytes", ctypes.c_uint64),
+                ("pool_used", ctypes.c_uint64), ("busy_s", ctypes.c_double)]
+
+
+POA_SERVER_QUEUED, POA_SERVER_RUNNING, POA_SERVER_DONE, POA_SERVER_FAILED, POA_SERVER_PARKED = range(5)
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [("cells", ctypes.c_uint64), ("reads", ctypes.c_uint64), ("device_ms", ctypes.c_double),
                 ("launches", ctypes.c_int32), ("relaunches", ctypes.c_int32), ("slots", ctypes.c_int32),
@@ -74,6 +88,15 @@ SIGNATURES = {
     "poa_batch_tune": (ctypes.c_int, [_vp, _vp, _i32, _u64]),
     "poa_align_noalloc": (ctypes.c_int, [_vp, _cp, _vp, _vp, _i64, _vp, _i64, _vp]),
     "poa_batch_transfer_bytes": (ctypes.c_int, [_vp, _vp, P(_u64), P(_u64)]),
+    "poa_server_create": (ctypes.c_int, [_vp, _cp, _u64, _i32, P(_vp)]),
+    "poa_server_submit": (ctypes.c_int, [_vp, _vp, _i64, P(_u8p), P(_i64), P(_i64)]),
+    "poa_server_wait": (ctypes.c_int, [_vp, _vp, _i64, ctypes.c_double, P(_i32)]),
+    "poa_server_job_info": (ctypes.c_int, [_vp, _vp, _i64, P(ServerJobInfo)]),
+    "poa_server_output": (ctypes.c_int, [_vp, _vp, _i64, _i32, _ccp, _ccp, P(ctypes.c_char_p), P(_i64)]),
+    "poa_server_release": (ctypes.c_int, [_vp, _vp, _i64]),
+    "poa_server_stats_get": (ctypes.c_int, [_vp, _vp, P(ServerStats)]),
+    "poa_server_tune": (ctypes.c_int, [_vp, _vp, ctypes.c_double]),
+    "poa_server_destroy": (None, [_vp]),
 }
 
 _lib = None

@@ -356,3 +356,72 @@ class Batch:
         h = ctypes.c_void_p()
         self.ctx.check(self.L.poa_batch_graph(self.ctx.h, self.h, s, ctypes.byref(h)))
         return Graph(ctx=self.ctx, handle=h)
+
+
+class Server:
+    """Serving loop over the C ABI (poa_server_*): jobs (read sets) are
+    submitted at any time and run with continuous batching on the device;
+    each finished job's graph stays resident until released. Safe to use
+    from several threads (submit on one, wait on others)."""
+
+    def __init__(self, params: Params, ctx: Optional[Context] = None, pool_bytes: int = 0, streams: int = 0):
+        self.ctx = ctx or default_context()
+        self.L = self.ctx.L
+        self.params = params
+        self._c, self._keep = params.to_c()
+        h = ctypes.c_void_p()
+        self.ctx.check(self.L.poa_server_create(self.ctx.h, ctypes.byref(self._c), pool_bytes, streams,
+                                                ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.poa_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, reads: Seq[bytes]) -> int:
+        arr, lens, _bufs = _seq_arrays([_bytes(r) for r in reads])
+        job = ctypes.c_int64()
+        self.ctx.check(self.L.poa_server_submit(self.ctx.h, self.h, len(reads), arr, lens, ctypes.byref(job)))
+        return job.value
+
+    def wait(self, job: int, timeout_ms: float = -1.0) -> int:
+        st = ctypes.c_int32()
+        self.ctx.check(self.L.poa_server_wait(self.ctx.h, self.h, job, float(timeout_ms), ctypes.byref(st)))
+        return st.value
+
+    def info(self, job: int) -> _lib.ServerJobInfo:
+        out = _lib.ServerJobInfo()
+        self.ctx.check(self.L.poa_server_job_info(self.ctx.h, self.h, job, ctypes.byref(out)))
+        return out
+
+    def output(self, job: int, result: int, sequences: Optional[Seq[Sequence]] = None) -> str:
+        out = ctypes.c_char_p()
+        n = ctypes.c_int64()
+        names = comments = None
+        if sequences is not None:
+            names = (ctypes.c_char_p * max(1, len(sequences)))(*[x.name.encode() for x in sequences])
+            comments = (ctypes.c_char_p * max(1, len(sequences)))(*[x.comment.encode() for x in sequences])
+        self.ctx.check(self.L.poa_server_output(self.ctx.h, self.h, job, result, names, comments, ctypes.byref(out),
+                                                ctypes.byref(n)))
+        try:
+            return ctypes.string_at(out, n.value).decode()
+        finally:
+            self.L.poa_free(ctypes.cast(out, ctypes.c_void_p))
+
+    def release(self, job: int) -> None:
+        self.ctx.check(self.L.poa_server_release(self.ctx.h, self.h, job))
+
+    def tune(self, arena_scale: float) -> None:
+        self.ctx.check(self.L.poa_server_tune(self.ctx.h, self.h, float(arena_scale)))
+
+    def stats(self) -> _lib.ServerStats:
+        out = _lib.ServerStats()
+        self.ctx.check(self.L.poa_server_stats_get(self.ctx.h, self.h, ctypes.byref(out)))
+        return out
