@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--mem-budget-gb", type=float, default=0.0,
                     help="device memory budget of the context (0: 90%% of free memory)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (small profiling runs)")
+    ap.add_argument("--serve-jobs", type=int, default=1024, help="jobs of the serving loop's saturation run (0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=12.0, help="length of the serving run at 80%% load")
     return ap.parse_args()
 
 
@@ -181,6 +183,70 @@ def cpu_baseline(sets, params, seconds: float):
     }
 
 
+def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006):
+    """Serving loop (continuous batching) on jobs drawn from the batched
+    workload's distribution: saturated throughput (all jobs submitted at
+    once), then Poisson arrivals at 80% of it, with each job's latency from
+    submission to completion (measured by the server)."""
+    import random
+
+    from minipoa_b200 import workloads
+
+    jobs = workloads.batched_sets(n_jobs, seed=seed)
+    server = mp.Server(params, ctx=ctx)
+    t0 = time.perf_counter()
+    ids = [server.submit(j) for j in jobs]
+    cells = 0
+    for i in ids:
+        server.wait(i)
+        cells += server.info(i).cells
+    sat_s = time.perf_counter() - t0
+    for i in ids:
+        server.release(i)
+    sat_rate = n_jobs / sat_s
+    rate = 0.8 * sat_rate
+    rng = random.Random(seed)
+    submitted, lat, load_cells = [], [], [0]
+    done = threading.Event()
+
+    def reaper():
+        k = 0
+        while not (done.is_set() and k >= len(submitted)):
+            if k >= len(submitted):
+                time.sleep(0.0005)
+                continue
+            j = submitted[k]
+            server.wait(j)
+            info = server.info(j)
+            lat.append(info.latency_ms)
+            load_cells[0] += info.cells
+            server.release(j)
+            k += 1
+
+    th = threading.Thread(target=reaper)
+    th.start()
+    t0 = time.perf_counter()
+    t_next = t0
+    while t_next - t0 < seconds:
+        now = time.perf_counter()
+        if now < t_next:
+            time.sleep(min(t_next - now, 0.002))
+            continue
+        submitted.append(server.submit(jobs[rng.randrange(n_jobs)]))
+        t_next += rng.expovariate(rate)
+    done.set()
+    th.join()
+    span = time.perf_counter() - t0
+    server.close()
+    lat.sort()
+    pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None  # noqa: E731
+    return {"workload": f"{n_jobs} jobs drawn like the batched workload (seed {seed})",
+            "saturated_jobs_per_s": sat_rate, "saturated_gcups": cells / sat_s / 1e9,
+            "load": "Poisson arrivals at 80% of the saturated job rate", "arrival_jobs_per_s": rate,
+            "jobs": len(lat), "gcups": load_cells[0] / span / 1e9,
+            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None}
+
+
 def load_traffic():
     """DRAM bytes per launch of the batched kernel from the committed ncu
     summary, scaled to this run's cells (null when absent)."""
@@ -297,6 +363,10 @@ def main():
                 "traffic": None if traffic is None else traffic.get("bytes_per_cell", 0) * cells / max(
                     1, sum(1 + s.relaunches for s in steps))}
 
+    serving = None
+    if rank == 0 and args.serve_jobs > 0:
+        serving = serving_bench(mp, params, ctx, args.serve_jobs, args.serve_seconds)
+
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(sets, params, args.cpu_seconds)
@@ -317,6 +387,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clock_info,
             "plain_vs_batched": plain,
+            "serving": serving,
         }
         print(json.dumps(line))
     if pg is not None:
