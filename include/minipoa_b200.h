@@ -178,6 +178,42 @@ int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *r
 int poa_align_noalloc(poa_ctx *ctx, const poa_params *params, poa_graph *graph, const uint8_t *d_query, int64_t len,
                       poa_aligned_base *d_out, int64_t out_cap, int64_t *d_out_len);
 
+/* ---- seed windows for seeded alignment (-S), host only (no context).
+ * Outputs are released with poa_free. Minimizer selection is this library's
+ * (forward ntHash, leftmost minimum); the reference takes it from the
+ * simd-minimizers crate, so the chosen k-mers can differ. Everything after
+ * the sketch follows src/minimizer.rs. */
+typedef struct poa_minimizer {
+  uint64_t value;  /* exact packed k-mer: A0 C1 T2 G3, first base in the low bits */
+  int64_t end;     /* inclusive position of its last base */
+  int64_t span;
+} poa_minimizer;
+typedef struct poa_anchor {
+  int64_t target_end;
+  int64_t query_end;
+  int64_t span;
+  int32_t adaptive_before;
+  int32_t reserved;
+} poa_anchor;
+/* sketch (src/minimizer.rs:39-75). */
+int poa_seed_sketch(const uint8_t *seq, int64_t len, int64_t k, int64_t w, poa_minimizer **out, int64_t *n);
+/* repeat_intervals (src/minimizer.rs:79-110): *n_out (start, end) pairs. */
+int poa_seed_repeat_intervals(const poa_minimizer *mm, int64_t n, int64_t len, int64_t max_dist, int64_t **out_pairs,
+                              int64_t *n_out);
+/* collect_anchors (src/minimizer.rs:128-172). */
+int poa_seed_collect_anchors(const poa_params *params, const uint8_t *query, int64_t qlen, const uint8_t *target,
+                             int64_t tlen, poa_anchor **out, int64_t *n);
+/* chain (src/minimizer.rs:199-366). */
+int poa_seed_chain(const poa_anchor *anchors, int64_t n, int64_t k, poa_anchor **out, int64_t *n_out);
+/* partition_windows (src/minimizer.rs:371-457). */
+int poa_seed_partition_windows(const poa_anchor *chain, int64_t n, int64_t tlen, int64_t qlen, int64_t max_drift,
+                               int64_t max_win, poa_anchor **out, int64_t *n_out, int32_t *tail_adaptive);
+/* anchor_windows (src/minimizer.rs:466-479): the windows align::align uses
+ * with seeding (src/align.rs:99-164), which poa_align, poa_align_sequences
+ * and poa_extend_graph run when params->seeding is set. */
+int poa_seed_anchor_windows(const poa_params *params, const uint8_t *query, int64_t qlen, const uint8_t *consensus,
+                            int64_t clen, poa_anchor **out, int64_t *n_out, int32_t *tail_adaptive);
+
 /* ---- batched independent read sets (no reference counterpart: the
  * reference runs one set per process; each set here is one extend_graph). */
 typedef struct poa_batch_stats {

@@ -21,6 +21,7 @@
 #include "host_graph.h"
 #include "poa_internal.h"
 #include "poa_pack.h"
+#include "seed.h"
 
 using namespace poa;
 
@@ -486,7 +487,6 @@ std::vector<poa_aligned_base> align_path(poa_ctx *ctx, const HostParams &hp, poa
                                          int64_t len, int mode, int64_t beg, int64_t end, int adaptive,
                                          uint64_t band_b, int kernel, int retry) {
   if (len < 0 || len > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
-  if (mode == 0 && hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
   DevParams P = ctx->params(hp);
   P.kernel = kernel;
   ctx->ensure_qbuf(size_t(len) + 16);
@@ -522,6 +522,87 @@ std::vector<poa_aligned_base> align_path(poa_ctx *ctx, const HostParams &hp, poa
   std::vector<poa_aligned_base> out(it.size());
   for (size_t k = 0; k < it.size(); ++k) out[k] = {it[k].x, it[k].y, it[k].z};
   return out;
+}
+
+// align::align with seeding (src/align.rs:99-164): the graph's consensus, the
+// seed windows of the query against it (host), then one banded alignment per
+// window between its anchor nodes (device) and the anchor nodes themselves,
+// in window order. Anchors that are not usable as hard constraints, or no
+// anchors at all, fall back to the whole graph with an adaptive band.
+std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const uint8_t *q,
+                                           int64_t len) {
+  g->sync();
+  std::vector<poa_aligned_base> out;
+  if (g->h.n_nodes <= 2) {
+    out.push_back({0, hp.encode('N'), -1});
+    for (int64_t c = 0; c < len; ++c) out.push_back({-1, hp.encode(q[c]), -1});
+    return out;
+  }
+  HostGraph hg = g->download();
+  std::vector<uint8_t> cons;
+  std::vector<int64_t> ids, cov;
+  hg.consensus(hp, cons, ids, cov);
+  const auto aw = anchor_windows(hp, q, len, cons.data(), int64_t(cons.size()));
+  auto whole = [&] { return align_path(ctx, hp, g, q, len, 1, 0, 1, 1, hp.b, 0, 1); };
+  if (aw.first.empty()) return whole();
+  struct Window {
+    int64_t beg, end, qbeg, qend;
+    bool adaptive;
+    int64_t a0, a1;  // anchor node ids: ids[a0..a1)
+  };
+  std::vector<Window> windows;
+  int64_t beg = 0, qbeg = 0, prev_t = -1;
+  for (const Anchor &a : aw.first) {
+    if (a.target_end + 1 < a.span) throw AlignError{POA_ERR_ALIGN, "invalid minimizer target span"};
+    if (a.query_end + 1 < a.span) throw AlignError{POA_ERR_ALIGN, "invalid minimizer query span"};
+    const int64_t ts = a.target_end + 1 - a.span, qs = a.query_end + 1 - a.span;
+    bool valid = a.span > 0 && a.target_end < int64_t(ids.size()) && a.query_end < len && qs >= qbeg &&
+                 (prev_t < 0 || ts > prev_t);
+    for (int64_t o = 0; valid && o < a.span; ++o)
+      valid = hp.encode(cons[size_t(ts + o)]) == hp.encode(q[qs + o]);
+    if (!valid) return whole();
+    windows.push_back({beg, ids[size_t(ts)], qbeg, qs, a.adaptive_before, ts, a.target_end});
+    beg = ids[size_t(a.target_end)];
+    qbeg = a.query_end + 1;
+    prev_t = a.target_end;
+  }
+  windows.push_back({beg, 1, qbeg, len, aw.second, 0, 0});
+  for (const Window &w : windows) {
+    auto part = align_path(ctx, hp, g, q + w.qbeg, w.qend - w.qbeg, 1, w.beg, w.end, w.adaptive ? 1 : 0,
+                           w.adaptive ? hp.b : hp.win_band, 0, 1);
+    out.insert(out.end(), part.begin(), part.end());
+    for (int64_t t = w.a0; t < w.a1; ++t) out.push_back({ids[size_t(t)], hg.base[size_t(ids[size_t(t)])], -1});
+  }
+  return out;
+}
+
+// extend_graph (src/lib.rs:184-204) with seeding: per read, the seeded path,
+// then add_path and the LIFO toposort on the device.
+void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::vector<const uint8_t *> &seqs,
+                   const std::vector<int64_t> &lens, int64_t r0) {
+  if (hp.progressive && r0 == 0) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
+  const int64_t n = int64_t(seqs.size());
+  int64_t total = 0;
+  for (int64_t r = r0; r < n; ++r) {
+    if (lens[size_t(r)] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+    total += lens[size_t(r)];
+  }
+  g->reserve(total + 2 * (n - r0), 2 * (total + 3 * (n - r0)), total + (n - r0), n - r0);
+  const DevParams P = ctx->params(hp);
+  for (int64_t r = r0; r < n; ++r) {
+    auto path = seeded_align(ctx, hp, g, seqs[size_t(r)], lens[size_t(r)]);
+    std::vector<int4> it(path.size());
+    for (size_t k = 0; k < path.size(); ++k)
+      it[k] = make_int4(int(path[k].node), int(path[k].base), int(path[k].aligned), 0);
+    ctx->ensure_items(it.size() + 4);
+    if (!it.empty())
+      CK(cudaMemcpyAsync(ctx->items, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_add_path(g->d_job, P, int(r), ctx->items, int(it.size()), ctx->stream));
+    g->check_status();
+    ctx->ensure_arena(std::max<int64_t>(int64_t(g->h.n_nodes) * 8 + 64, int64_t(64) << 20));
+    CK(launch_toposort(g->d_job, ctx->arena, ctx->arena_bytes, ctx->stream));
+    g->check_status();
+  }
 }
 
 std::vector<std::string> name_list(int64_t n, const char *const *names, const char *prefix) {
@@ -717,7 +798,10 @@ int poa_align_sequences(poa_ctx *ctx, const poa_params *params, int64_t n_seqs, 
     std::unique_ptr<poa_graph> g(new_graph(ctx, hp, c));
     std::vector<const uint8_t *> s(seqs, seqs + n_seqs);
     std::vector<int64_t> l(lens, lens + n_seqs);
-    extend_range(ctx, hp, g.get(), s, l, 0);
+    if (hp.seeding)
+      seeded_extend(ctx, hp, g.get(), s, l, 0);
+    else
+      extend_range(ctx, hp, g.get(), s, l, 0);
     *out = g.release();
   });
 }
@@ -730,7 +814,10 @@ int poa_extend_graph(poa_ctx *ctx, const poa_params *params, poa_graph *graph, i
     if (existing > 0) ap.progressive = false;
     std::vector<const uint8_t *> s(seqs, seqs + n_seqs);
     std::vector<int64_t> l(lens, lens + n_seqs);
-    extend_range(ctx, ap, graph, s, l, existing);
+    if (ap.seeding)
+      seeded_extend(ctx, ap, graph, s, l, existing);
+    else
+      extend_range(ctx, ap, graph, s, l, existing);
   });
 }
 
@@ -740,7 +827,9 @@ int poa_align(poa_ctx *ctx, const poa_params *params, poa_graph *graph, const ui
   *out_len = 0;
   return api(ctx, [&] {
     HostParams hp = checked_params(params);
-    auto v = align_path(ctx, hp, graph, query, len, 0, 0, 1, 0, hp.b, 0, 1);
+    if (len < 0 || len > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+    auto v = hp.seeding ? seeded_align(ctx, hp, graph, query, len)
+                        : align_path(ctx, hp, graph, query, len, 0, 0, 1, 0, hp.b, 0, 1);
     *out = (poa_aligned_base *)std::malloc(sizeof(poa_aligned_base) * (v.size() + 1));
     std::memcpy(*out, v.data(), v.size() * sizeof(poa_aligned_base));
     *out_len = int64_t(v.size());

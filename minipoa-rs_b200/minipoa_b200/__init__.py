@@ -8,5 +8,6 @@ Server admits read sets as they arrive (continuous batching).
 """
 from .params import AlignedBase, CParams, Params, Sequence, default_matrix  # noqa: F401
 from .api import (  # noqa: F401
-    Batch, Context, Graph, PoaError, Server, align, align_sequences, default_context, dp_backend, extend_graph, poa, run,
+    Anchor, Batch, Context, Graph, Minimizer, PoaError, Server, align, anchor_windows, chain, collect_anchors,
+    partition_windows, repeat_intervals, sketch, align_sequences, default_context, dp_backend, extend_graph, poa, run,
 )

@@ -26,6 +26,15 @@ class GraphSizes(ctypes.Structure):
                 ("n_rank", ctypes.c_int64)]
 
 
+class MinimizerC(ctypes.Structure):
+    _fields_ = [("value", ctypes.c_uint64), ("end", ctypes.c_int64), ("span", ctypes.c_int64)]
+
+
+class AnchorC(ctypes.Structure):
+    _fields_ = [("target_end", ctypes.c_int64), ("query_end", ctypes.c_int64), ("span", ctypes.c_int64),
+                ("adaptive_before", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class ServerJobInfo(ctypes.Structure):
     _fields_ = [("state", ctypes.c_int32), ("reserved", ctypes.c_int32), ("cells", ctypes.c_uint64),
                 ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
@@ -96,6 +105,13 @@ SIGNATURES = {
     "poa_server_release": (ctypes.c_int, [_vp, _vp, _i64]),
     "poa_server_stats_get": (ctypes.c_int, [_vp, _vp, P(ServerStats)]),
     "poa_server_tune": (ctypes.c_int, [_vp, _vp, ctypes.c_double]),
+    "poa_seed_sketch": (ctypes.c_int, [_u8p, _i64, _i64, _i64, P(P(MinimizerC)), P(_i64)]),
+    "poa_seed_repeat_intervals": (ctypes.c_int, [P(MinimizerC), _i64, _i64, _i64, P(P(_i64)), P(_i64)]),
+    "poa_seed_collect_anchors": (ctypes.c_int, [_cp, _u8p, _i64, _u8p, _i64, P(P(AnchorC)), P(_i64)]),
+    "poa_seed_chain": (ctypes.c_int, [P(AnchorC), _i64, _i64, P(P(AnchorC)), P(_i64)]),
+    "poa_seed_partition_windows": (ctypes.c_int, [P(AnchorC), _i64, _i64, _i64, _i64, _i64, P(P(AnchorC)), P(_i64),
+                                                  P(_i32)]),
+    "poa_seed_anchor_windows": (ctypes.c_int, [_cp, _u8p, _i64, _u8p, _i64, P(P(AnchorC)), P(_i64), P(_i32)]),
     "poa_server_destroy": (None, [_vp]),
 }
 

@@ -5,6 +5,7 @@ on the B200; this module only marshals arguments and results.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from typing import List, Optional, Sequence as Seq, Tuple
 
 from . import _lib
@@ -425,3 +426,109 @@ class Server:
         out = _lib.ServerStats()
         self.ctx.check(self.L.poa_server_stats_get(self.ctx.h, self.h, ctypes.byref(out)))
         return out
+
+
+# ---- seed windows (src/minimizer.rs), host only ----------------------------
+
+@dataclasses.dataclass(frozen=True)
+class Minimizer:
+    value: int
+    end: int
+    span: int
+
+
+@dataclasses.dataclass(frozen=True)
+class Anchor:
+    target_end: int
+    query_end: int
+    span: int
+    adaptive_before: bool = False
+
+
+def _u8(data: bytes):
+    buf = ctypes.create_string_buffer(bytes(data) or b"\0", max(1, len(data)))
+    return ctypes.cast(buf, ctypes.POINTER(ctypes.c_uint8)), buf
+
+
+def _take(L, ptr, n, conv):
+    try:
+        return [conv(ptr[k]) for k in range(n)]
+    finally:
+        L.poa_free(ctypes.cast(ptr, ctypes.c_void_p))
+
+
+def _anchor(a) -> Anchor:
+    return Anchor(a.target_end, a.query_end, a.span, bool(a.adaptive_before))
+
+
+def _anchors_c(anchors: Seq[Anchor]):
+    arr = (_lib.AnchorC * max(1, len(anchors)))()
+    for k, a in enumerate(anchors):
+        arr[k] = _lib.AnchorC(a.target_end, a.query_end, a.span, int(a.adaptive_before), 0)
+    return arr
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise PoaError(rc, "invalid arguments")
+
+
+def sketch(seq: bytes, k: int, w: int) -> List[Minimizer]:
+    """minimizer::sketch (src/minimizer.rs:39-75)."""
+    L = _lib.load()
+    p, _keep = _u8(seq)
+    out, n = ctypes.POINTER(_lib.MinimizerC)(), ctypes.c_int64()
+    _check(L.poa_seed_sketch(p, len(seq), k, w, ctypes.byref(out), ctypes.byref(n)))
+    return _take(L, out, n.value, lambda m: Minimizer(m.value, m.end, m.span))
+
+
+def repeat_intervals(mm: Seq[Minimizer], length: int, max_dist: int) -> List[Tuple[int, int]]:
+    """minimizer::repeat_intervals (src/minimizer.rs:79-110)."""
+    L = _lib.load()
+    arr = (_lib.MinimizerC * max(1, len(mm)))(*[_lib.MinimizerC(m.value, m.end, m.span) for m in mm])
+    out, n = ctypes.POINTER(ctypes.c_int64)(), ctypes.c_int64()
+    _check(L.poa_seed_repeat_intervals(arr, len(mm), length, max_dist, ctypes.byref(out), ctypes.byref(n)))
+    flat = _take(L, out, 2 * n.value, int)
+    return [(flat[2 * i], flat[2 * i + 1]) for i in range(n.value)]
+
+
+def collect_anchors(params: Params, query: bytes, target: bytes) -> List[Anchor]:
+    """minimizer::collect_anchors (src/minimizer.rs:128-172)."""
+    L = _lib.load()
+    c, _k = params.to_c()
+    q, _kq = _u8(query)
+    t, _kt = _u8(target)
+    out, n = ctypes.POINTER(_lib.AnchorC)(), ctypes.c_int64()
+    _check(L.poa_seed_collect_anchors(ctypes.byref(c), q, len(query), t, len(target), ctypes.byref(out),
+                                      ctypes.byref(n)))
+    return _take(L, out, n.value, _anchor)
+
+
+def chain(anchors: Seq[Anchor], k: int) -> List[Anchor]:
+    """minimizer::chain (src/minimizer.rs:199-366)."""
+    L = _lib.load()
+    out, n = ctypes.POINTER(_lib.AnchorC)(), ctypes.c_int64()
+    _check(L.poa_seed_chain(_anchors_c(anchors), len(anchors), k, ctypes.byref(out), ctypes.byref(n)))
+    return _take(L, out, n.value, _anchor)
+
+
+def partition_windows(chain_: Seq[Anchor], tlen: int, qlen: int, max_drift: int,
+                      max_win: int) -> Tuple[List[Anchor], bool]:
+    """minimizer::partition_windows (src/minimizer.rs:371-457)."""
+    L = _lib.load()
+    out, n, tail = ctypes.POINTER(_lib.AnchorC)(), ctypes.c_int64(), ctypes.c_int32()
+    _check(L.poa_seed_partition_windows(_anchors_c(chain_), len(chain_), tlen, qlen, max_drift, max_win,
+                                        ctypes.byref(out), ctypes.byref(n), ctypes.byref(tail)))
+    return _take(L, out, n.value, _anchor), bool(tail.value)
+
+
+def anchor_windows(params: Params, query: bytes, consensus: bytes) -> Tuple[List[Anchor], bool]:
+    """minimizer::anchor_windows (src/minimizer.rs:466-479)."""
+    L = _lib.load()
+    c, _k = params.to_c()
+    q, _kq = _u8(query)
+    t, _kt = _u8(consensus)
+    out, n, tail = ctypes.POINTER(_lib.AnchorC)(), ctypes.c_int64(), ctypes.c_int32()
+    _check(L.poa_seed_anchor_windows(ctypes.byref(c), q, len(query), t, len(consensus), ctypes.byref(out),
+                                     ctypes.byref(n), ctypes.byref(tail)))
+    return _take(L, out, n.value, _anchor), bool(tail.value)
