@@ -198,9 +198,10 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
     ids = [server.submit(j) for j in jobs]
     cells = 0
     for i in ids:
-        server.wait(i)
+        server.wait(i, 120000.0)
         cells += server.info(i).cells
     sat_s = time.perf_counter() - t0
+    print(f"[bench] serving: {n_jobs} jobs at once in {sat_s:.2f} s", file=sys.stderr, flush=True)
     for i in ids:
         server.release(i)
     sat_rate = n_jobs / sat_s
@@ -216,7 +217,7 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
                 time.sleep(0.0005)
                 continue
             j = submitted[k]
-            server.wait(j)
+            server.wait(j, 120000.0)
             info = server.info(j)
             lat.append(info.latency_ms)
             load_cells[0] += info.cells
@@ -237,6 +238,8 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
     done.set()
     th.join()
     span = time.perf_counter() - t0
+    print(f"[bench] serving: {len(submitted)} Poisson arrivals at {rate:.0f}/s, drained in {span:.2f} s",
+          file=sys.stderr, flush=True)
     server.close()
     lat.sort()
     pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None  # noqa: E731
@@ -365,7 +368,10 @@ def main():
 
     serving = None
     if rank == 0 and args.serve_jobs > 0:
-        serving = serving_bench(mp, params, ctx, args.serve_jobs, args.serve_seconds)
+        try:
+            serving = serving_bench(mp, params, ctx, args.serve_jobs, args.serve_seconds)
+        except Exception as e:  # the throughput line above stands on its own
+            serving = {"error": str(e)}
 
     cb = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -1577,7 +1577,9 @@ void poa_server::finish_wave(Wave &w) {
   finish_jobs();  // flags raised just before the wave ended
   std::lock_guard<std::mutex> lk(mu);
   for (int64_t id : w.ids) {
-    ServerJob &sj = *jobs.at(id);
+    auto it = jobs.find(id);
+    if (it == jobs.end()) continue;  // finished early and already released by its caller
+    ServerJob &sj = *it->second;
     sj.d_desc = nullptr;
     if (sj.state != POA_SERVER_PARKED) continue;
     // the graph is intact at its next read; come back with twice the arena
