@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (small profiling runs)")
     ap.add_argument("--serve-jobs", type=int, default=1024, help="jobs of the serving loop's saturation run (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="length of the serving run at 80%% load")
+    ap.add_argument("--seeded-reads", type=int, default=20,
+                    help="reads of the seeded-window run (16.5 kbp ancestor, ~5%% error; 0: skip)")
     return ap.parse_args()
 
 
@@ -250,6 +252,34 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
             "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None}
 
 
+def seeded_bench(mp, ctx, n_reads: int, seed: int = 1002):
+    """Seeded windowed POA (-S -B -r1) on a 16.5 kbp ancestor with reads at
+    about 5% error (3/1/1% sub/ins/del, indel lengths geometric with mean
+    1.5): windows/s with all windows of a read in one launch (one warp per
+    window) and with one launch per window, on the same reads."""
+    from minipoa_b200 import workloads
+    from minipoa_b200.params import Params
+
+    reads = workloads.seeded_window_set(seed)[:n_reads]
+    params = Params(seeding=True, adaptive=True, result=1)
+    out = {"workload": f"16,500 bp ancestor, first {len(reads)} of 100 reads (seed {seed}), -S -B -r1"}
+    msa = {}
+    for name, plain in (("batched", False), ("plain", True)):
+        ctx.tune_windows(plain)
+        w0 = ctx.window_stats()
+        t0 = time.perf_counter()
+        g = mp.align_sequences(params, reads, ctx=ctx)
+        dt = time.perf_counter() - t0
+        w1 = ctx.window_stats()
+        msa[name] = g.msa(params, [mp.Sequence(name=f"read{i}", seq=r) for i, r in enumerate(reads)])
+        out[name] = {"windows": w1[0] - w0[0], "launches": w1[1] - w0[1], "fallback_reads": w1[2] - w0[2],
+                     "seconds": dt, "windows_per_s": (w1[0] - w0[0]) / dt, "reads_per_s": len(reads) / dt}
+    ctx.tune_windows(False)
+    out["identical_msa"] = msa["batched"] == msa["plain"]
+    out["batched_over_plain"] = out["batched"]["windows_per_s"] / out["plain"]["windows_per_s"]
+    return out
+
+
 def load_traffic():
     """DRAM bytes per launch of the batched kernel from the committed ncu
     summary, scaled to this run's cells (null when absent)."""
@@ -373,6 +403,13 @@ def main():
         except Exception as e:  # the throughput line above stands on its own
             serving = {"error": str(e)}
 
+    seeded = None
+    if rank == 0 and args.seeded_reads > 0:
+        try:
+            seeded = seeded_bench(mp, ctx, args.seeded_reads)
+        except Exception as e:
+            seeded = {"error": str(e)}
+
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(sets, params, args.cpu_seconds)
@@ -394,6 +431,7 @@ def main():
             "clocks": clock_info,
             "plain_vs_batched": plain,
             "serving": serving,
+            "seeded": seeded,
         }
         print(json.dumps(line))
     if pg is not None:

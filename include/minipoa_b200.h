@@ -89,6 +89,14 @@ void poa_ctx_destroy(poa_ctx *ctx);
 const char *poa_last_error(const poa_ctx *ctx);
 void poa_free(void *ptr);
 
+/* Seeded reads (params->seeding): the seed windows of a read are aligned in
+ * one launch, one warp per window (0, default), or one launch per window (1).
+ * Same results; the second form is the reference-shaped one. */
+int poa_ctx_tune_windows(poa_ctx *ctx, int32_t one_launch_per_window);
+/* Seeded reads so far on this context: windows aligned, kernel launches
+ * for them, and reads that fell back to the whole graph (no usable anchors). */
+int poa_ctx_window_stats(poa_ctx *ctx, uint64_t *windows, uint64_t *launches, uint64_t *fallbacks);
+
 /* Params::validate (src/lib.rs:149-173). */
 int poa_params_validate(poa_ctx *ctx, const poa_params *params);
 

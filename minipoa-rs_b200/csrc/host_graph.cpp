@@ -303,3 +303,37 @@ bool HostGraph::gfa(const HostParams &p, const std::vector<std::string> &names, 
 }
 
 }  // namespace poa
+
+namespace poa {
+
+// graph.rs:125-178 with grouped = false, as the device toposort: in-degrees
+// from the incoming lists, zero-degree nodes pushed in id order, successors
+// in outgoing order.
+int32_t HostGraph::lifo_order() {
+  std::vector<int32_t> deg(static_cast<size_t>(n)), stack;
+  stack.reserve(size_t(n));
+  for (int id = 0; id < n; ++id) {
+    deg[size_t(id)] = int32_t(in_off[size_t(id) + 1] - in_off[size_t(id)]);
+    if (deg[size_t(id)] == 0) stack.push_back(id);
+  }
+  rank.assign(size_t(n), 0);
+  rank_to_node.clear();
+  while (!stack.empty()) {
+    const int id = stack.back();
+    stack.pop_back();
+    rank[size_t(id)] = int32_t(rank_to_node.size());
+    rank_to_node.push_back(id);
+    for (int64_t k = out_off[size_t(id)]; k < out_off[size_t(id) + 1]; ++k) {
+      const int next = out_id[size_t(k)];
+      if (deg[size_t(next)] == 0) {
+        n_rank = int(rank_to_node.size());
+        return 13;  // column dependencies (graph.rs:164-166)
+      }
+      if (--deg[size_t(next)] == 0) stack.push_back(next);
+    }
+  }
+  n_rank = int(rank_to_node.size());
+  return n_rank == n ? 0 : 12;  // cycle (graph.rs:174-176)
+}
+
+}  // namespace poa

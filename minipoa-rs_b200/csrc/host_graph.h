@@ -50,6 +50,10 @@ struct HostGraph {
   bool msa(const HostParams &p, const std::vector<std::string> &names, const std::vector<std::string> &comments,
            std::string &out, std::string &err) const;
   bool gfa(const HostParams &p, const std::vector<std::string> &names, std::string &out, std::string &err) const;
+  // LIFO Kahn order (graph.rs:125-178 with grouped = false) into rank /
+  // rank_to_node; 0 or the device status code of the failure (cycle, column
+  // dependencies).
+  int32_t lifo_order();
   // Column-grouped LIFO Kahn ranks (graph.rs:125-178 with grouped = true).
   bool grouped_ranks(std::vector<int32_t> &node_rank, std::vector<int32_t> &order, std::string &err) const;
 };

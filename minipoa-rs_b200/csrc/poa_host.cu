@@ -173,6 +173,8 @@ struct poa_ctx {
   int32_t *d_matrix = nullptr;
   uint8_t *d_encode = nullptr;
   size_t matrix_cap = 0;
+  int window_launch = 0;  // seeded reads: 0 = one launch for all windows, 1 = one launch per window
+  uint64_t seed_windows = 0, seed_launches = 0, seed_fallbacks = 0;
 
   void *dalloc(size_t bytes) {
     if (allocated + bytes > budget) throw AlignError{POA_ERR_ALLOC, "device memory budget exceeded"};
@@ -530,7 +532,7 @@ std::vector<poa_aligned_base> align_path(poa_ctx *ctx, const HostParams &hp, poa
 // in window order. Anchors that are not usable as hard constraints, or no
 // anchors at all, fall back to the whole graph with an adaptive band.
 std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const uint8_t *q,
-                                           int64_t len) {
+                                           int64_t len, bool ranks_stale = false) {
   g->sync();
   std::vector<poa_aligned_base> out;
   if (g->h.n_nodes <= 2) {
@@ -539,11 +541,27 @@ std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, p
     return out;
   }
   HostGraph hg = g->download();
+  if (ranks_stale) {
+    // the previous read's toposort (graph.rs:125-178), on the downloaded copy
+    const int32_t st = hg.lifo_order();
+    if (st != ST_OK) throw AlignError{status_code(st), status_message(st, 0, 0)};
+    const size_t n = size_t(hg.n);
+    CK(cudaMemcpyAsync(g->h.rank, hg.rank.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(g->h.rank_to_node, hg.rank_to_node.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    g->sync();
+    g->h.n_rank = hg.n_rank;
+    g->h.order_exact = 1;
+    g->upload();
+  }
   std::vector<uint8_t> cons;
   std::vector<int64_t> ids, cov;
   hg.consensus(hp, cons, ids, cov);
   const auto aw = anchor_windows(hp, q, len, cons.data(), int64_t(cons.size()));
-  auto whole = [&] { return align_path(ctx, hp, g, q, len, 1, 0, 1, 1, hp.b, 0, 1); };
+  auto whole = [&] {
+    ++ctx->seed_fallbacks;
+    ++ctx->seed_launches;
+    return align_path(ctx, hp, g, q, len, 1, 0, 1, 1, hp.b, 0, 1);
+  };
   if (aw.first.empty()) return whole();
   struct Window {
     int64_t beg, end, qbeg, qend;
@@ -567,17 +585,81 @@ std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, p
     prev_t = a.target_end;
   }
   windows.push_back({beg, 1, qbeg, len, aw.second, 0, 0});
-  for (const Window &w : windows) {
-    auto part = align_path(ctx, hp, g, q + w.qbeg, w.qend - w.qbeg, 1, w.beg, w.end, w.adaptive ? 1 : 0,
-                           w.adaptive ? hp.b : hp.win_band, 0, 1);
-    out.insert(out.end(), part.begin(), part.end());
+  const int nw = int(windows.size());
+  ctx->seed_windows += uint64_t(nw);
+  std::vector<std::vector<poa_aligned_base>> parts(static_cast<size_t>(nw));
+  std::vector<char> done(size_t(nw), 0);
+  if (ctx->window_launch == 0 && nw > 1) {
+    // all windows of the read in one launch, one warp each
+    std::vector<int4> win(static_cast<size_t>(nw));
+    std::vector<uint64_t> band(static_cast<size_t>(nw));
+    std::vector<int64_t> item_off(size_t(nw) + 1, 0);
+    for (int k = 0; k < nw; ++k) {
+      const Window &w = windows[size_t(k)];
+      const int64_t ql = w.qend - w.qbeg;
+      win[size_t(k)] = make_int4(int(w.beg), int(w.end), int(w.qbeg), int(ql) | (w.adaptive ? int(0x80000000u) : 0));
+      band[size_t(k)] = w.adaptive ? hp.b : hp.win_band;
+      item_off[size_t(k) + 1] = item_off[size_t(k)] + ql + 8;
+    }
+    auto r256 = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o_win = r256(size_t(len) + 16), o_band = o_win + r256(size_t(nw) * 16),
+                 o_off = o_band + r256(size_t(nw) * 8), o_n = o_off + r256(size_t(nw + 1) * 8),
+                 o_st = o_n + r256(size_t(nw) * 4), total = o_st + r256(size_t(nw) * 4);
+    ctx->ensure_qbuf(total);
+    ctx->ensure_items(size_t(item_off.back()) + 4);
+    ctx->ensure_arena(std::max<int64_t>(ctx->arena_bytes, int64_t(nw) * (int64_t(32) << 20)));
+    const int64_t slot = ctx->arena_bytes / nw / 256 * 256;
+    uint8_t *qb = ctx->qbuf;
+    if (len) CK(cudaMemcpyAsync(qb, q, size_t(len), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(qb + o_win, win.data(), size_t(nw) * 16, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(qb + o_band, band.data(), size_t(nw) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(qb + o_off, item_off.data(), size_t(nw + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    const DevParams P = ctx->params(hp);
+    ++ctx->seed_launches;
+    CK(launch_windows(g->d_job, P, ctx->arena, slot, nw, reinterpret_cast<const int4 *>(qb + o_win),
+                      reinterpret_cast<const uint64_t *>(qb + o_band), qb, ctx->items,
+                      reinterpret_cast<const int64_t *>(qb + o_off), reinterpret_cast<int32_t *>(qb + o_n),
+                      reinterpret_cast<int32_t *>(qb + o_st), ctx->stream));
+    std::vector<int32_t> on(static_cast<size_t>(nw)), ost(static_cast<size_t>(nw));
+    std::vector<int4> it(static_cast<size_t>(item_off.back()));
+    CK(cudaMemcpyAsync(on.data(), qb + o_n, size_t(nw) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ost.data(), qb + o_st, size_t(nw) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(it.data(), ctx->items, it.size() * sizeof(int4), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < nw; ++k) {
+      const int32_t st = ost[size_t(k)];
+      if (st == ST_ARENA_FULL) continue;  // aligned again below, with a growing arena
+      if (st != ST_OK) {
+        g->sync();
+        throw AlignError{status_code(st), status_message(st, g->h.err_i, g->h.err_j)};
+      }
+      auto &pk = parts[size_t(k)];
+      for (int32_t t = 0; t < on[size_t(k)]; ++t) {
+        const int4 x = it[size_t(item_off[size_t(k)] + t)];
+        pk.push_back({x.x, x.y, x.z});
+      }
+      done[size_t(k)] = 1;
+    }
+  }
+  for (int k = 0; k < nw; ++k) {
+    if (done[size_t(k)]) continue;
+    const Window &w = windows[size_t(k)];
+    ++ctx->seed_launches;
+    parts[size_t(k)] = align_path(ctx, hp, g, q + w.qbeg, w.qend - w.qbeg, 1, w.beg, w.end, w.adaptive ? 1 : 0,
+                                  w.adaptive ? hp.b : hp.win_band, 0, 1);
+  }
+  for (int k = 0; k < nw; ++k) {
+    const Window &w = windows[size_t(k)];
+    out.insert(out.end(), parts[size_t(k)].begin(), parts[size_t(k)].end());
     for (int64_t t = w.a0; t < w.a1; ++t) out.push_back({ids[size_t(t)], hg.base[size_t(ids[size_t(t)])], -1});
   }
   return out;
 }
 
 // extend_graph (src/lib.rs:184-204) with seeding: per read, the seeded path,
-// then add_path and the LIFO toposort on the device.
+// then add_path on the device; the LIFO toposort of each step runs on the
+// host copy the next read downloads anyway (its consensus needs it), and on
+// the device after the last read.
 void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::vector<const uint8_t *> &seqs,
                    const std::vector<int64_t> &lens, int64_t r0) {
   if (hp.progressive && r0 == 0) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
@@ -589,8 +671,9 @@ void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::
   }
   g->reserve(total + 2 * (n - r0), 2 * (total + 3 * (n - r0)), total + (n - r0), n - r0);
   const DevParams P = ctx->params(hp);
+  bool stale = false;
   for (int64_t r = r0; r < n; ++r) {
-    auto path = seeded_align(ctx, hp, g, seqs[size_t(r)], lens[size_t(r)]);
+    auto path = seeded_align(ctx, hp, g, seqs[size_t(r)], lens[size_t(r)], stale);
     std::vector<int4> it(path.size());
     for (size_t k = 0; k < path.size(); ++k)
       it[k] = make_int4(int(path[k].node), int(path[k].base), int(path[k].aligned), 0);
@@ -599,6 +682,9 @@ void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::
       CK(cudaMemcpyAsync(ctx->items, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
     CK(launch_add_path(g->d_job, P, int(r), ctx->items, int(it.size()), ctx->stream));
     g->check_status();
+    stale = true;
+  }
+  if (stale) {
     ctx->ensure_arena(std::max<int64_t>(int64_t(g->h.n_nodes) * 8 + 64, int64_t(64) << 20));
     CK(launch_toposort(g->d_job, ctx->arena, ctx->arena_bytes, ctx->stream));
     g->check_status();
@@ -768,6 +854,20 @@ void poa_ctx_destroy(poa_ctx *ctx) {
 // failed poa_ctx_create.
 const char *poa_last_error(const poa_ctx *ctx) { return ctx ? t_last_error.c_str() : g_create_error.c_str(); }
 void poa_free(void *ptr) { std::free(ptr); }
+
+int poa_ctx_tune_windows(poa_ctx *ctx, int32_t one_launch_per_window) {
+  if (!ctx || one_launch_per_window < 0 || one_launch_per_window > 1) return POA_ERR_INVALID;
+  ctx->window_launch = one_launch_per_window;
+  return POA_OK;
+}
+
+int poa_ctx_window_stats(poa_ctx *ctx, uint64_t *windows, uint64_t *launches, uint64_t *fallbacks) {
+  if (!ctx || !windows || !launches || !fallbacks) return POA_ERR_INVALID;
+  *windows = ctx->seed_windows;
+  *launches = ctx->seed_launches;
+  *fallbacks = ctx->seed_fallbacks;
+  return POA_OK;
+}
 
 int poa_params_validate(poa_ctx *ctx, const poa_params *params) {
   return api(ctx, [&] { checked_params(params); });

@@ -25,6 +25,10 @@ cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, i
 cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q, int qlen,
                          int mode, int beg_id, int end_id, int adaptive, uint64_t band_b, int retry, int4 *out,
                          int32_t *out_n, cudaStream_t stream);
+// One warp per seed window of a read (win: beg, end, qbeg, qlen | adaptive << 31).
+cudaError_t launch_windows(Job *job_dev, const DevParams &P, char *arenas, int64_t slot_bytes, int n_win,
+                           const int4 *win, const uint64_t *band, const uint8_t *query, int4 *items,
+                           const int64_t *item_off, int32_t *out_n, int32_t *out_st, cudaStream_t stream);
 cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, int4 *items, int n,
                             cudaStream_t stream);
 cudaError_t launch_add_node(Job *job_dev, int sigma, int base, cudaStream_t stream);

@@ -178,6 +178,37 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
   }
 }
 
+// The seed windows of one read (align.rs:99-164), one warp per window: warp w
+// aligns query[qbeg, qbeg + qlen) between anchor nodes beg (included) and
+// end (excluded) with the full-DP retry, in its own arena slice, and writes
+// its path to items[item_off[w] ...]. The graph is only read.
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
+    k_windows(Job *J, DevParams P, char *arenas, int64_t slot_bytes, int n_win, const int4 *win,
+              const uint64_t *band, const uint8_t *query, int4 *items, const int64_t *item_off, int32_t *out_n,
+              int32_t *out_st) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n_win) return;
+  const int4 d = win[w];  // (beg, end, qbeg, qlen | adaptive << 31)
+  const bool adaptive = (unsigned(d.w) >> 31) != 0;
+  const int qlen = d.w & 0x7fffffff;
+  Scratch s;
+  int n_items = 0;
+  Work cells{};
+  const int32_t st = poa_retry(J, P, arenas + w * slot_bytes, slot_bytes, d.x, d.y, query + d.z, qlen, adaptive,
+                               band[w], s, &n_items, &cells, warp_smem());
+  if (st == ST_OK)
+    for (int k = lane; k < n_items; k += 32) items[item_off[w] + k] = s.items[k];
+  if (lane == 0) {
+    out_n[w] = st == ST_OK ? n_items : 0;
+    out_st[w] = st;
+    if (st == ST_OK) {
+      atomicAdd(reinterpret_cast<unsigned long long *>(&J->cells), (unsigned long long)cells.cells);
+      atomicAdd(reinterpret_cast<unsigned long long *>(&J->dp_bytes), (unsigned long long)cells.dp_bytes);
+    }
+  }
+}
+
 __global__ void k_add_path(Job *J, DevParams P, int seq_id, int4 *items, int n) {
   int32_t st = ST_OK;
   if (!add_path_warp(J, P, seq_id, items, n, &st) && threadIdx.x == 0) st = add_path(J, P, seq_id, items, n);
@@ -275,6 +306,22 @@ cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t 
                          int32_t *out_n, cudaStream_t stream) {
   k_align<<<1, 32, sizeof(WarpSmem), stream>>>(job_dev, P, arena, bytes, q, qlen, mode, beg_id, end_id, adaptive,
                                                band_b, retry, out, out_n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_windows(Job *job_dev, const DevParams &P, char *arenas, int64_t slot_bytes, int n_win,
+                           const int4 *win, const uint64_t *band, const uint8_t *query, int4 *items,
+                           const int64_t *item_off, int32_t *out_n, int32_t *out_st, cudaStream_t stream) {
+  const size_t smem = WARPS_PER_BLOCK * sizeof(WarpSmem);
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(k_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int blocks = (n_win + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+  k_windows<<<blocks, WARPS_PER_BLOCK * 32, smem, stream>>>(job_dev, P, arenas, slot_bytes, n_win, win, band, query,
+                                                            items, item_off, out_n, out_st);
   return cudaGetLastError();
 }
 

@@ -68,6 +68,8 @@ SIGNATURES = {
     "poa_dp_backend": (ctypes.c_char_p, []),
     "poa_ctx_create": (ctypes.c_int, [ctypes.c_int, _u64, P(_vp)]),
     "poa_ctx_destroy": (None, [_vp]),
+    "poa_ctx_tune_windows": (ctypes.c_int, [_vp, _i32]),
+    "poa_ctx_window_stats": (ctypes.c_int, [_vp, P(_u64), P(_u64), P(_u64)]),
     "poa_last_error": (ctypes.c_char_p, [_vp]),
     "poa_free": (None, [_vp]),
     "poa_params_validate": (ctypes.c_int, [_vp, _cp]),

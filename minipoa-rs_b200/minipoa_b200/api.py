@@ -64,6 +64,18 @@ class Context:
         if rc != 0:
             raise PoaError(rc, self.L.poa_last_error(self.h).decode())
 
+    def tune_windows(self, one_launch_per_window: bool) -> None:
+        """Seeded reads: align a read's seed windows in one launch (False,
+        default) or one launch per window (True)."""
+        self.check(self.L.poa_ctx_tune_windows(self.h, int(bool(one_launch_per_window))))
+
+    def window_stats(self) -> Tuple[int, int, int]:
+        """(windows aligned, launches for them, whole-graph fallbacks) of the
+        seeded reads run on this context so far."""
+        w, la, fb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self.check(self.L.poa_ctx_window_stats(self.h, ctypes.byref(w), ctypes.byref(la), ctypes.byref(fb)))
+        return w.value, la.value, fb.value
+
     def validate(self, params: Params) -> Optional[str]:
         c, keep = params.to_c()
         rc = self.L.poa_params_validate(self.h, ctypes.byref(c))

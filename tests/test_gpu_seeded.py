@@ -93,3 +93,26 @@ def test_seeded_align_of_one_query_matches_oracle(mp, oracle):
     short = reads[3][:30]
     got = [(a.node, a.base, a.aligned) for a in mp.align(params, g, short)]
     assert got == seeded_path(mp, o, params, short)
+
+
+def test_windows_in_one_launch_equal_one_launch_per_window(mp):
+    from minipoa_b200 import workloads
+
+    rng = np.random.default_rng(11)
+    reads = workloads.read_set(rng, 4000, 5, 0.03, 0.01, 0.01, indel_mean=1.5)
+    params = Params(seeding=True, adaptive=True)
+    ctx = mp.default_context()
+    w0 = ctx.window_stats()
+    ctx.tune_windows(False)
+    batched = mp.align_sequences(params, reads).dump()
+    w1 = ctx.window_stats()
+    ctx.tune_windows(True)
+    try:
+        plain = mp.align_sequences(params, reads).dump()
+    finally:
+        ctx.tune_windows(False)
+    w2 = ctx.window_stats()
+    assert batched == plain
+    # same windows both ways; far fewer launches in the batched form
+    assert w1[0] - w0[0] == w2[0] - w1[0] > 4
+    assert w1[1] - w0[1] < w2[1] - w1[1]
