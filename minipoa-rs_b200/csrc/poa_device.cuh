@@ -299,9 +299,10 @@ __device__ inline int32_t add_path(Job *J, const DevParams &P, int seq_id, int4 
 
 // add_path (graph.rs:82-122) by the whole warp, one item per lane. It covers
 // the case every alignment path is in: the items name pairwise distinct
-// nodes. That holds when the pre-existing nodes of the path have strictly
-// increasing ranks, no item names the sink, and no two items create the same
-// column sibling (same parent and base); those three facts are checked first,
+// nodes. That holds when no pre-existing node is named twice (checked with
+// `mark`, n_nodes zeroed words of scratch, or, without scratch, by strictly
+// increasing ranks), no item names the sink, and no two items create the
+// same column sibling (same parent and base); those facts are checked first,
 // and when one fails nothing has been changed and false is returned, so the
 // caller runs the serial add_path. With distinct nodes every node gains at
 // most one incoming and one outgoing edge, so the edges are independent and
@@ -310,7 +311,8 @@ __device__ inline int32_t add_path(Job *J, const DevParams &P, int seq_id, int4 
 // another order than the serial loop numbers them; chunk numbers are storage
 // only, the lists keep their insertion order. Invalid items and capacity
 // give the serial function's status (true is returned, graph unchanged).
-__device__ inline bool add_path_warp(Job *J, const DevParams &P, int seq_id, int4 *items, int n, int32_t *status) {
+__device__ inline bool add_path_warp(Job *J, const DevParams &P, int seq_id, int4 *items, int n, int32_t *status,
+                                     int32_t *mark = nullptr) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int n_old = J->n_nodes;
@@ -340,6 +342,10 @@ __device__ inline bool add_path_warp(Job *J, const DevParams &P, int seq_id, int
   // column sibling, whose (parent, base) slot of `aligned` is claimed)
   bool ok = true;
   int rank_carry = -1;
+  if (mark) {
+    for (int v = lane; v < n_old; v += 32) mark[v] = 0;
+    __syncwarp();
+  }
   for (int t0 = 0; t0 < n; t0 += 32) {
     const int t = t0 + lane;
     int w = -1, rk = -1;
@@ -360,7 +366,10 @@ __device__ inline bool add_path_warp(Job *J, const DevParams &P, int seq_id, int
         }
       }
       if (w >= 0) {
-        rk = J->rank[w];
+        if (mark)
+          fail = fail || atomicExch(&mark[w], 1) != 0;  // named twice
+        else
+          rk = J->rank[w];
         fail = fail || w == 1;
       }
       items[t].w = w;
@@ -374,7 +383,7 @@ __device__ inline bool add_path_warp(Job *J, const DevParams &P, int seq_id, int
     int before = __shfl_up_sync(FULL, pm, 1);
     if (lane == 0) before = -1;
     before = max(before, rank_carry);
-    if (w >= 0 && rk <= before) fail = true;
+    if (!mark && w >= 0 && rk <= before) fail = true;
     rank_carry = max(rank_carry, __shfl_sync(FULL, pm, 31));
     if (__any_sync(FULL, fail)) ok = false;
   }
@@ -688,89 +697,89 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
     }
     return L;
   };
+  // One pass (forward: predecessors, head; backward: successors, tail): per
+  // row, the first predecessor (successor) of largest weight, ties to the
+  // larger support, among those whose value is set. Rows with at most two
+  // candidates (nearly all) read both candidates' values before choosing,
+  // and the next row's list entries are taken by shuffle while this row
+  // computes.
+  auto pass = [&](bool forward, int64_t *val, const int32_t *st, const int32_t *ct, int2 *ent) {
+    const int first = forward ? 1 : n - 2;
+    const int step = forward ? 1 : -1;
+    const int count = n - 1;  // rows 1..n-1 forward, n-2..0 backward
+    auto row_of = [&](int q) { return first + step * q; };
+    Lists nxt = load(st, ct, ent, row_of(lane), lane < count);
+    for (int q0 = 0; q0 < count; q0 += 32) {
+      const Lists cur = nxt;
+      nxt = load(st, ct, ent, row_of(q0 + 32 + lane), q0 + 32 + lane < count);
+      const int lim = min(32, count - q0);
+      int lb = __shfl_sync(FULL, cur.start, 0), lc = __shfl_sync(FULL, cur.cnt, 0);
+      int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, 0), __shfl_sync(FULL, cur.e0.y, 0));
+      int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, 0), __shfl_sync(FULL, cur.e1.y, 0));
+      for (int k = 0; k < lim; ++k) {
+        const int i = row_of(q0 + k);
+        const int pb = lb, pc = lc;
+        const int2 e0 = f0, e1 = f1;
+        const int kn = k + 1 < lim ? k + 1 : k;  // the next row's entries, fetched early
+        lb = __shfl_sync(FULL, cur.start, kn);
+        lc = __shfl_sync(FULL, cur.cnt, kn);
+        f0 = make_int2(__shfl_sync(FULL, cur.e0.x, kn), __shfl_sync(FULL, cur.e0.y, kn));
+        f1 = make_int2(__shfl_sync(FULL, cur.e1.x, kn), __shfl_sync(FULL, cur.e1.y, kn));
+        auto get = [&](int x, int64_t &v, int64_t &sp) {
+          const bool near = (forward ? i - x : x - i) < GRING;
+          v = near ? rv[x & (GRING - 1)] : val[x];
+          sp = near ? rsu[x & (GRING - 1)] : s.support[x];
+        };
+        bool have = false;
+        int bw = 0;
+        int64_t bsup = 0, bval = 0;
+        auto consider = [&](const int2 &e, int64_t v, int64_t sp, int t) {
+          if (v == NEG64) {
+            if (forward) ent[pb + t].x = -1;
+            return;
+          }
+          if (!have || e.y > bw || (e.y == bw && sp > bsup)) {
+            have = true;
+            bw = e.y;
+            bsup = sp;
+            bval = v;
+          }
+        };
+        if (pc <= 2) {
+          int64_t v0 = NEG64, s0 = 0, v1 = NEG64, s1 = 0;
+          if (pc >= 1) get(e0.x, v0, s0);
+          if (pc >= 2) get(e1.x, v1, s1);
+          if (pc >= 1) consider(e0, v0, s0, 0);
+          if (pc >= 2) consider(e1, v1, s1, 1);
+        } else {
+          for (int t = 0; t < pc; ++t) {
+            const int2 e = t == 0 ? e0 : (t == 1 ? e1 : ent[pb + t]);
+            int64_t v, sp;
+            get(e.x, v, sp);
+            consider(e, v, sp, t);
+          }
+        }
+        const int64_t vi = have ? bval + 1 : NEG64;
+        const int64_t si = have ? bsup + bw : 0;
+        if (have) {
+          val[i] = vi;
+          s.support[i] = si;
+        }
+        rv[i & (GRING - 1)] = vi;
+        rsu[i & (GRING - 1)] = si;
+      }
+    }
+  };
   // forward: head along the heaviest (then most supported) predecessor
   s.head[0] = 0;
   rv[0] = 0;
   rsu[0] = 0;
-  Lists nxt = load(s.pred_start, s.pred_cnt, s.pred, 1 + lane, 1 + lane < n);
-  for (int i0 = 1; i0 < n; i0 += 32) {
-    const Lists cur = nxt;
-    nxt = load(s.pred_start, s.pred_cnt, s.pred, i0 + 32 + lane, i0 + 32 + lane < n);
-    const int lim = min(32, n - i0);
-    for (int k = 0; k < lim; ++k) {
-      const int i = i0 + k;
-      const int pb = __shfl_sync(FULL, cur.start, k), pc = __shfl_sync(FULL, cur.cnt, k);
-      const int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, k), __shfl_sync(FULL, cur.e0.y, k));
-      const int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, k), __shfl_sync(FULL, cur.e1.y, k));
-      bool have = false;
-      int bw = 0;
-      int64_t bsup = 0, bhead = 0;
-      for (int t = 0; t < pc; ++t) {
-        const int2 e = t == 0 ? f0 : (t == 1 ? f1 : s.pred[pb + t]);
-        const bool near = i - e.x < GRING;
-        const int64_t hp = near ? rv[e.x & (GRING - 1)] : s.head[e.x];
-        if (hp == NEG64) {
-          s.pred[pb + t].x = -1;
-          continue;
-        }
-        const int64_t sp = near ? rsu[e.x & (GRING - 1)] : s.support[e.x];
-        if (!have || e.y > bw || (e.y == bw && sp > bsup)) {
-          have = true;
-          bw = e.y;
-          bsup = sp;
-          bhead = hp;
-        }
-      }
-      const int64_t hi = have ? bhead + 1 : NEG64;
-      const int64_t si = have ? bsup + bw : 0;
-      if (have) {
-        s.head[i] = hi;
-        s.support[i] = si;
-      }
-      rv[i & (GRING - 1)] = hi;
-      rsu[i & (GRING - 1)] = si;
-    }
-  }
+  pass(true, s.head, s.pred_start, s.pred_cnt, s.pred);
   // backward: tail along the heaviest (then most supported) successor; the
   // support array continues from the forward pass
   s.tail[n - 1] = 1;
   rv[(n - 1) & (GRING - 1)] = 1;  // rsu keeps the forward support of the last row
-  nxt = load(s.succ_start, s.succ_cnt, s.succ, n - 2 - lane, n - 2 - lane >= 0);
-  for (int i0 = n - 2; i0 >= 0; i0 -= 32) {
-    const Lists cur = nxt;
-    nxt = load(s.succ_start, s.succ_cnt, s.succ, i0 - 32 - lane, i0 - 32 - lane >= 0);
-    const int lim = min(32, i0 + 1);
-    for (int k = 0; k < lim; ++k) {
-      const int i = i0 - k;
-      const int sb = __shfl_sync(FULL, cur.start, k), sn = __shfl_sync(FULL, cur.cnt, k);
-      const int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, k), __shfl_sync(FULL, cur.e0.y, k));
-      const int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, k), __shfl_sync(FULL, cur.e1.y, k));
-      bool have = false;
-      int bw = 0;
-      int64_t bsup = 0, btail = 0;
-      for (int t = 0; t < sn; ++t) {
-        const int2 e = t == 0 ? f0 : (t == 1 ? f1 : s.succ[sb + t]);
-        const bool near = e.x - i < GRING;
-        const int64_t ts = near ? rv[e.x & (GRING - 1)] : s.tail[e.x];
-        if (ts == NEG64) continue;
-        const int64_t ss = near ? rsu[e.x & (GRING - 1)] : s.support[e.x];
-        if (!have || e.y > bw || (e.y == bw && ss > bsup)) {
-          have = true;
-          bw = e.y;
-          bsup = ss;
-          btail = ts;
-        }
-      }
-      const int64_t ti = have ? btail + 1 : NEG64;
-      const int64_t si = have ? bsup + bw : 0;
-      if (have) {
-        s.tail[i] = ti;
-        s.support[i] = si;
-      }
-      rv[i & (GRING - 1)] = ti;
-      rsu[i & (GRING - 1)] = si;
-    }
-  }
+  pass(false, s.tail, s.succ_start, s.succ_cnt, s.succ);
   __syncwarp();
   return s.head[n - 1] == NEG64 ? ST_NO_PATH : ST_OK;
 }
@@ -1939,7 +1948,8 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, sm);
   if (st != ST_OK) return st;
   const int n_old = J->n_nodes;
-  if (!add_path_warp(J, P, r, s.items, n_items, &st)) {
+  int32_t *mark = s.dp_bytes >= int64_t(n_old) * 4 ? reinterpret_cast<int32_t *>(s.dp) : nullptr;
+  if (!add_path_warp(J, P, r, s.items, n_items, &st, mark)) {
     if (lane == 0) st = add_path(J, P, r, s.items, n_items);
     st = __shfl_sync(FULL, st, 0);
   }
