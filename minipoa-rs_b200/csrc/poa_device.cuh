@@ -1051,7 +1051,15 @@ constexpr int RING_CAP = 2560;
 constexpr int RING_MAX_LEN = 512;  // widest band computed by the striped row
 constexpr int SMEM_MATRIX = 512;   // sigma^2 entries kept in shared memory (sigma <= 22)
 constexpr int SEQ_SMEM = 5632;     // padded query columns kept in shared memory
+// Where a warp's ring lives: its own ring_m / ring_d by default; a warp
+// running alone in its block may take the other warps' shared memory.
+struct RingView {
+  int32_t *m, *d;
+  int cap;     // entries per state, a multiple of 8
+  int pad[3];  // pad[0]: this warp leads cooperative rows (see CoopDesc)
+};
 struct WarpSmem {
+  RingView rv;
   int32_t ring_m[RING_CAP];
   int32_t ring_d[RING_CAP];
   int32_t matrix[SMEM_MATRIX];
@@ -1060,11 +1068,24 @@ struct WarpSmem {
   uint8_t seq8[SEQ_SMEM];
 };
 
+// Every kernel sets its warp's ring to the warp's own arrays first.
+__device__ inline void ring_default(WarpSmem *sm) {
+  if ((threadIdx.x & 31) == 0) {
+    sm->rv.m = sm->ring_m;
+    sm->rv.d = sm->ring_d;
+    sm->rv.cap = RING_CAP;
+    sm->rv.pad[0] = 0;  // no cooperative rows
+    sm->rv.pad[1] = 0;
+    sm->rv.pad[2] = 0;
+  }
+  __syncwarp();
+}
+
 // Ring entry of column j of a row whose band starts at `start` and whose
-// first column sits at ring entry `pos`.
-__device__ __forceinline__ int ring_at(int pos, int start, int j) {
+// first column sits at ring entry `pos`, in a ring of `cap` entries.
+__device__ __forceinline__ int ring_at(int pos, int start, int j, int cap) {
   const int x = pos + (j - start);
-  return x >= RING_CAP ? x - RING_CAP : x;
+  return x >= cap ? x - cap : x;
 }
 
 // One int32 DP row of at most 128*G columns (align.rs:751-828) in stripes:
@@ -1084,7 +1105,8 @@ template <int G, bool ADAPT>
 __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                                const int32_t *mrow, int32_t E, int32_t O, unsigned vmask,
                                                int my_ps, int my_pl, int my_pos, const int32_t *my_g,
-                                               WarpSmem *sm, int pos_i, int32_t &bestv, int &bestj) {
+                                               int32_t *rm, int32_t *rd, int cap, int pos_i, int32_t &bestv,
+                                               int &bestj) {
   const int stop = start + len;
   int32_t Mx[G][4], Dx[G][4];
 #pragma unroll
@@ -1109,10 +1131,10 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
       for (int g = 0; g < G; ++g) {
         const int j0 = start + 128 * g + 4 * lane;
         in[g] = j0 < stop && j0 >= ps && j0 < ps + pl;
-        const int x = ring_at(pos, ps, in[g] ? j0 : ps);
-        m4[g] = *reinterpret_cast<const int4 *>(sm->ring_m + x);
-        d4[g] = *reinterpret_cast<const int4 *>(sm->ring_d + x);
-        prev[g] = sm->ring_m[x == 0 ? RING_CAP - 1 : x - 1];
+        const int x = ring_at(pos, ps, in[g] ? j0 : ps, cap);
+        m4[g] = *reinterpret_cast<const int4 *>(rm + x);
+        d4[g] = *reinterpret_cast<const int4 *>(rd + x);
+        prev[g] = rm[x == 0 ? cap - 1 : x - 1];
       }
     } else {
 #pragma unroll
@@ -1198,9 +1220,9 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
           }
       }
       const int o = j0 - start;
-      const int x = ring_at(pos_i, start, j0);
-      *reinterpret_cast<int4 *>(sm->ring_m + x) = make_int4(mv[0], mv[1], mv[2], mv[3]);
-      *reinterpret_cast<int4 *>(sm->ring_d + x) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
+      const int x = ring_at(pos_i, start, j0, cap);
+      *reinterpret_cast<int4 *>(rm + x) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+      *reinterpret_cast<int4 *>(rd + x) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
       *reinterpret_cast<int4 *>(R + o) = make_int4(mv[0], mv[1], mv[2], mv[3]);
       *reinterpret_cast<int4 *>(R + len + o) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
       *reinterpret_cast<int4 *>(R + 2 * len + o) = make_int4(iv[0], iv[1], iv[2], iv[3]);
@@ -1212,36 +1234,172 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
 template <bool ADAPT>
 __device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                             const int32_t *mrow, int32_t E, int32_t O, unsigned vmask, int ps,
-                                            int pl, int pos, const int32_t *g, WarpSmem *sm, int pos_i, int32_t &bv,
-                                            int &bj) {
+                                            int pl, int pos, const int32_t *g, int32_t *rm, int32_t *rd, int cap,
+                                            int pos_i, int32_t &bv, int &bj) {
   if (len <= 128)
-    dp_row_striped<1, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
+    dp_row_striped<1, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
   else if (len <= 256)
-    dp_row_striped<2, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
+    dp_row_striped<2, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
   else if (len <= 384)
-    dp_row_striped<3, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
+    dp_row_striped<3, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
   else
-    dp_row_striped<4, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, sm, pos_i, bv, bj);
+    dp_row_striped<4, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative rows. A warp running a giant job alone in its block (the other
+// warps of the block would otherwise idle) has three of them compute its DP
+// rows with it: stripe 0 of every row by the leader, stripes 1-3 by the
+// helpers. The leader publishes
+// each row in shared memory; the four warps meet at named barrier 1 three
+// times per row (row published, stripe aggregates published, row written)
+// and at barrier 2 at the start of every row loop and once when the job is
+// done. The arithmetic is the single-warp striped row's: the stripe carries
+// compose as carry[g+1] = max(aggregate[g], carry[g] + 128E).
+constexpr int COOP_ROWS = 0, COOP_DONE = 1;  // phase modes
+constexpr int COOP_ROW = 0, COOP_STOP = 1;   // row operations
+struct CoopDesc {
+  int mode, op, start, len, pos_i, n_pred, cap, pad0;
+  int32_t E, O, pad1, pad2;
+  int32_t *R;
+  const int32_t *mrow;
+  const uint8_t *q8;
+  int32_t *rm, *rd;
+  int32_t agg[4];
+  int ps[32], pl[32], pos[32];
+  const int32_t *g[32];
+};
+static_assert(sizeof(CoopDesc) <= sizeof(int32_t) * RING_CAP, "CoopDesc must fit a ring array");
+
+__device__ __forceinline__ void coop_bar(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+// Stripe g of the published row (every warp of the block calls this once per
+// row, after barrier 1 has made the row visible).
+__device__ inline void coop_stripe(CoopDesc *c, int g) {
+  const int lane = threadIdx.x & 31;
+  const int start = c->start, len = c->len, stop = start + len, cap = c->cap;
+  const int32_t E = c->E, O = c->O;
+  int32_t *rm = c->rm, *rd = c->rd;
+  const int j0 = start + 128 * g + 4 * lane;
+  int32_t Mx[4], Dx[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    Mx[k] = NEG32;
+    Dx[k] = NEG32;
+  }
+  const int np = c->n_pred;
+  for (int t = 0; t < np; ++t) {
+    const int ps = c->ps[t], pl = c->pl[t], pos = c->pos[t];
+    const int32_t *gp = c->g[t];
+    const bool in = j0 < stop && j0 >= ps && j0 < ps + pl;
+    int4 m4, d4;
+    int32_t prev;
+    if (pos >= 0) {
+      const int x = ring_at(pos, ps, in ? j0 : ps, cap);
+      m4 = *reinterpret_cast<const int4 *>(rm + x);
+      d4 = *reinterpret_cast<const int4 *>(rd + x);
+      prev = rm[x == 0 ? cap - 1 : x - 1];
+    } else {
+      const int c0 = in ? j0 - ps : 0;
+      m4 = *reinterpret_cast<const int4 *>(gp + c0);
+      d4 = *reinterpret_cast<const int4 *>(gp + pl + c0);
+      prev = gp[c0 > 0 ? c0 - 1 : 0];
+    }
+    const int32_t pv = j0 > ps ? prev : NEG32;
+    if (in) {
+      Mx[0] = maxs(Mx[0], pv);
+      Mx[1] = maxs(Mx[1], m4.x);
+      Mx[2] = maxs(Mx[2], m4.y);
+      Mx[3] = maxs(Mx[3], m4.z);
+      Dx[0] = __viaddmax_s32(d4.x, E, __viaddmax_s32(m4.x, O, Dx[0]));
+      Dx[1] = __viaddmax_s32(d4.y, E, __viaddmax_s32(m4.y, O, Dx[1]));
+      Dx[2] = __viaddmax_s32(d4.z, E, __viaddmax_s32(m4.z, O, Dx[2]));
+      Dx[3] = __viaddmax_s32(d4.w, E, __viaddmax_s32(m4.w, O, Dx[3]));
+    }
+  }
+  constexpr int32_t BELOW = INT32_MIN / 2;
+  int32_t X[4];
+  const uint32_t bw = *reinterpret_cast<const uint32_t *>(c->q8 + min(j0, stop - 4));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int32_t prof = c->mrow[(bw >> (8 * k)) & 0xff];
+    Mx[k] = __viaddmax_s32(Mx[k], prof, Dx[k]);  // Mx now holds md
+    X[k] = k == 0 ? Mx[k] + O : __viaddmax_s32(X[k - 1], E, Mx[k] + O);
+  }
+  int32_t y = X[3];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) y = __viaddmax_s32(__shfl_up_sync(FULL, y, d), d * 4 * E, y);
+  int32_t pre = __shfl_up_sync(FULL, y, 1);
+  if (lane == 0) pre = BELOW;
+  const int32_t y31 = __shfl_sync(FULL, y, 31);
+  if (lane == 0) c->agg[g] = y31;
+  coop_bar(1);
+  int32_t carry = NEG32;
+  for (int h = 0; h < g; ++h) carry = __viaddmax_s32(carry, 128 * E, c->agg[h]);
+  const int32_t cin = __viaddmax_s32(carry, 4 * lane * E, pre);
+  if (j0 < stop) {
+    int32_t iv[4], mv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      iv[k] = k == 0 ? cin : __viaddmax_s32(cin, k * E, X[k - 1]);
+      mv[k] = maxs(Mx[k], iv[k]);
+    }
+    const int o = j0 - start;
+    const int x = ring_at(c->pos_i, start, j0, cap);
+    int32_t *R = c->R;
+    *reinterpret_cast<int4 *>(rm + x) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+    *reinterpret_cast<int4 *>(rd + x) = make_int4(Dx[0], Dx[1], Dx[2], Dx[3]);
+    *reinterpret_cast<int4 *>(R + o) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+    *reinterpret_cast<int4 *>(R + len + o) = make_int4(Dx[0], Dx[1], Dx[2], Dx[3]);
+    *reinterpret_cast<int4 *>(R + 2 * len + o) = make_int4(iv[0], iv[1], iv[2], iv[3]);
+  }
+  coop_bar(1);
+}
+
+// The block-mates' side: rows of every row loop the leader opens, until the
+// leader's job is done.
+__device__ inline void coop_helper(CoopDesc *c, int g) {
+  for (;;) {
+    coop_bar(2);
+    if (c->mode == COOP_DONE) {
+      coop_bar(2);  // every helper has read the mode before the leader reuses the descriptor
+      return;
+    }
+    for (;;) {
+      coop_bar(1);
+      if (c->op == COOP_STOP) break;
+      coop_stripe(c, g);
+    }
+  }
+}
+
+// Leader side of the release: the helpers leave coop_helper, and the
+// leader's ring is its own slice again (the descriptor's memory included).
+__device__ inline void coop_release(WarpSmem *sm) {
+  if ((threadIdx.x & 31) == 0) reinterpret_cast<CoopDesc *>(sm->ring_m)->mode = COOP_DONE;
+  coop_bar(2);
+  coop_bar(2);
+  ring_default(sm);
 }
 
 // Ring entry of a predecessor row's first column (arena offset `po`) while
 // row `off` is computed, or -1 when the row's states are no longer (or were
 // never) in the ring: intact while the rows written after it hold at most
 // RING_CAP entries. Arena offsets are 3x the cumulative band length.
-__device__ __forceinline__ int ring_pos(int64_t po, int64_t off, int64_t ring_floor) {
-  if (po < ring_floor || off - po > 3 * int64_t(RING_CAP)) return -1;
-  return int((po / 3) % RING_CAP);
+__device__ __forceinline__ int ring_pos(int64_t po, int64_t off, int64_t ring_floor, int cap) {
+  if (po < ring_floor || off - po > 3 * int64_t(cap)) return -1;
+  return int((po / 3) % cap);
 }
 
 // Copies row 0 (arena offset 0, computed serially) into the ring; returns the
 // ring floor (1 when the row is too wide to enter it).
 template <typename S>
-__device__ inline int64_t ring_put_row0(WarpSmem *sm, const S *A, int len) {
+__device__ inline int64_t ring_put_row0(int32_t *rm, int32_t *rd, const S *A, int len) {
   const int lane = threadIdx.x & 31;
   if (len > RING_MAX_LEN) return 1;
   for (int c = lane; c < len; c += 32) {
-    sm->ring_m[c] = int32_t(A[c]);
-    sm->ring_d[c] = int32_t(A[len + c]);
+    rm[c] = int32_t(A[c]);
+    rd[c] = int32_t(A[len + c]);
   }
   __syncwarp();
   return 0;
@@ -1336,7 +1494,7 @@ __device__ __forceinline__ int4 ld_early(const int4 *p) {
 // RING_CAP entries were written since), else -1, plus its arena offset. A row
 // goes through the ring when `ring` is set, its band is at most RING_MAX_LEN
 // and it has at most 32 predecessors (row 0: when its band fits).
-__device__ inline void plan_rows(Scratch &s, int n, bool ring) {
+__device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap) {
   const int lane = threadIdx.x & 31;
   int carry = 0;  // rows before this block that did not go through the ring
   for (int i0 = 0; i0 < n; i0 += 32) {
@@ -1348,7 +1506,7 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring) {
       const int64_t off = s.row_off[i];
       s.plan[i] = make_int4(s.row_start[i], len, s.pred_start[i], pc);
       s.plan2[i] = make_int4(int(uint64_t(off) & 0xffffffffu), int(uint64_t(off) >> 32), s.row_base[i],
-                             int((off / 3) % RING_CAP));
+                             int((off / 3) % cap));
     }
     const unsigned slow = __ballot_sync(FULL, i < n && !fast);
     if (i < n) s.nf[i] = carry + __popc(slow & ((1u << lane) - 1u));  // non-ring rows among 0..i-1
@@ -1362,7 +1520,7 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring) {
       const int4 m = s.pmeta[pb + t];
       const int64_t po = s.pmeta_off[pb + t];
       int pos = -1;
-      if (m.x >= 0 && m.z > 0 && s.nf[m.x] == nfi && off - po <= 3 * int64_t(RING_CAP)) pos = int((po / 3) % RING_CAP);
+      if (m.x >= 0 && m.z > 0 && s.nf[m.x] == nfi && off - po <= 3 * int64_t(cap)) pos = int((po / 3) % cap);
       s.pmeta2[pb + t] = make_int4(pos, int(uint64_t(po) & 0xffffffffu), int(uint64_t(po) >> 32), 0);
     }
   }
@@ -1438,6 +1596,9 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   const bool smem_matrix = P.sigma * P.sigma <= SMEM_MATRIX;
   // ring entries of rows before ring_floor (an arena offset) are not valid
   int64_t ring_floor = 0;
+  int32_t *const rm = sm ? sm->rv.m : nullptr;
+  int32_t *const rd = sm ? sm->rv.d : nullptr;
+  const int rcap = sm ? sm->rv.cap : RING_CAP;
   if (sm) {
     if (smem_matrix)
       for (int k = lane; k < P.sigma * P.sigma; k += 32) sm->matrix[k] = P.matrix[k];
@@ -1510,10 +1671,25 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     __syncwarp();
     fill_pmeta(s, n);
     const bool ring = kFastType && sm;
-    plan_rows(s, n, ring);
+    plan_rows(s, n, ring, rcap);
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
     __syncwarp();
-    if (ring) ring_put_row0(sm, A, s.row_len[0]);
+    if (ring) ring_put_row0(rm, rd, A, s.row_len[0]);
+    // a lone giant's block-mates join the row loop (cooperative rows)
+    const bool coop = ring && sm->rv.pad[0] != 0;
+    CoopDesc *cd = coop ? reinterpret_cast<CoopDesc *>(sm->ring_m) : nullptr;
+    if (coop) {
+      if (lane == 0) {
+        cd->mode = COOP_ROWS;
+        cd->E = int32_t(E);
+        cd->O = int32_t(O);
+        cd->q8 = q8;
+        cd->rm = rm;
+        cd->rd = rd;
+        cd->cap = rcap;
+      }
+      coop_bar(2);
+    }
     // rows 1..n-1, software-pipelined: row i+2's plan and row i+1's
     // predecessor entries are loaded while row i computes
     const int4 zero = make_int4(0, 0, 0, 0), none = make_int4(-1, 0, 0, 0);
@@ -1549,10 +1725,31 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + mo;
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
+        if (coop) {
+          const int slot = __popc(vmask & ((1u << lane) - 1u));
+          if (ok) {
+            cd->ps[slot] = mt.y;
+            cd->pl[slot] = mt.z;
+            cd->pos[slot] = mr.x;
+            cd->g[slot] = my_g;
+          }
+          if (lane == 0) {
+            cd->op = COOP_ROW;
+            cd->start = start;
+            cd->len = len;
+            cd->pos_i = b.w;
+            cd->n_pred = __popc(vmask);
+            cd->R = reinterpret_cast<int32_t *>(R);
+            cd->mrow = mrow;
+          }
+          coop_bar(1);
+          coop_stripe(cd, 0);  // the leader computes stripe 0
+          continue;
+        }
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
         dp_row_fast<false>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
-                           mt.y, mt.z, ok ? mr.x : -1, my_g, sm, b.w, bv, bj);
+                           mt.y, mt.z, ok ? mr.x : -1, my_g, rm, rd, rcap, b.w, bv, bj);
         __syncwarp();
         continue;
       }
@@ -1560,6 +1757,10 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
       int bj = INT32_MAX;
       dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, false, bv, bj);
       __syncwarp();
+    }
+    if (coop) {  // the block-mates leave the row loop
+      if (lane == 0) cd->op = COOP_STOP;
+      coop_bar(1);
     }
   } else {
     // Adaptive band (align.rs:711-729, 829-897): row i's band follows its
@@ -1607,7 +1808,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         }
         if (lane == 0) dp_row0<S>(R, len, s00, E, O);
         __syncwarp();
-        if (kFastType && sm) ring_floor = ring_put_row0(sm, A, len);
+        if (kFastType && sm) ring_floor = ring_put_row0(rm, rd, A, len);
         continue;
       }
       const int node = J->rank_to_node[beg + i];
@@ -1627,7 +1828,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
             const int64_t po = s.row_off[p];
             my_g = reinterpret_cast<const int32_t *>(A) + po;
             ok = my_pl > 0;
-            if (ok) my_pos = ring_pos(po, off, ring_floor);
+            if (ok) my_pos = ring_pos(po, off, ring_floor, rcap);
           }
         }
         const unsigned vmask = __ballot_sync(FULL, ok);
@@ -1635,7 +1836,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
         dp_row_fast<true>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
-                          my_ps, my_pl, my_pos, my_g, sm, int((off / 3) % RING_CAP), bv, bj);
+                          my_ps, my_pl, my_pos, my_g, rm, rd, rcap, int((off / 3) % rcap), bv, bj);
         bestv = S(bv);
         bestj = bj;
       } else {

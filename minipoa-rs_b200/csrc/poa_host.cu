@@ -1115,6 +1115,10 @@ int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *r
 
 // ---- batch
 
+// a job is giant when its estimated work is this many times the average
+// share of one resident warp
+constexpr double GIANT_FACTOR = 1.5;
+
 int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, const int64_t *set_off,
                      const uint8_t *const *seqs, const int64_t *lens, poa_batch **out) {
   *out = nullptr;
@@ -1209,14 +1213,18 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
       const double reads = double(set_off[s + 1] - set_off[s]);
       est[size_t(s)] = sum * std::min(w, mx + 16.0) * (1.0 + 0.03 * reads);
     }
-    // giant jobs: well above the per-warp share of the whole batch
-    const double share = std::accumulate(est.begin(), est.end(), 0.0) /
-                         double(std::max(1, ctx->sm_count * batch_resident_warps_per_sm()));
-    for (int64_t s = 0; s < n_sets; ++s) b->jobs[size_t(s)].giant = est[size_t(s)] > 1.5 * share ? 1 : 0;
-    b->upload_jobs();
     b->order.resize(size_t(n_sets));
     std::iota(b->order.begin(), b->order.end(), 0);
     std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return est[a] > est[c]; });
+    // giant jobs: well above the per-warp share of the whole batch, at most
+    // one per SM (the largest ones, which start first, one per SM)
+    const double share = std::accumulate(est.begin(), est.end(), 0.0) /
+                         double(std::max(1, ctx->sm_count * batch_resident_warps_per_sm()));
+    for (int64_t k = 0; k < std::min<int64_t>(n_sets, ctx->sm_count); ++k) {
+      const int32_t s = b->order[size_t(k)];
+      b->jobs[size_t(s)].giant = est[size_t(s)] > GIANT_FACTOR * share ? 1 : 0;
+    }
+    b->upload_jobs();
     b->d_order = (int32_t *)ctx->dalloc(b->order.size() * 4 + 4);
     b->d_queue = (int32_t *)ctx->dalloc(sched_words(b->jobs.size()) * 4);
     CK(cudaEventCreate(&b->e0));

@@ -10,11 +10,10 @@ namespace poa {
 
 // Launchers (poa_kernels.cu). All are asynchronous on `stream`.
 // `sched` holds sched_words(n_jobs) zeroed int32 words: the queue head, the
-// per-SM and per-level counters that spread the first jobs over the SMs, a
-// per-SM flag raised while the SM runs a giant job, and one claim flag per
-// queue position.
+// per-SM and per-level counters that spread the first jobs over the SMs, and
+// one claim flag per queue position.
 constexpr int SCHED_SM_SLOTS = 512, SCHED_LEVELS = 64;
-inline size_t sched_words(size_t n_jobs) { return 4 + 2 * SCHED_SM_SLOTS + SCHED_LEVELS + n_jobs; }
+inline size_t sched_words(size_t n_jobs) { return 4 + SCHED_SM_SLOTS + SCHED_LEVELS + n_jobs; }
 cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
                          const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream);
 cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,

@@ -6,10 +6,12 @@
 
 namespace poa {
 
-constexpr int WARPS_PER_BLOCK = 4;
-// Two 4-warp blocks of the batched kernel fit one SM's 228 KB of shared
-// memory (1 KB of it is reserved per block), matching __launch_bounds__.
-constexpr int BLOCKS_PER_SM = 2;
+constexpr int WARPS_PER_BLOCK = 8;
+// One 8-warp block of the batched kernel fills one SM's 228 KB of shared
+// memory (1 KB of it is reserved per block), matching __launch_bounds__; a
+// giant job alone on its SM then has the whole SM's shared memory as its ring
+// and three block-mates as helpers.
+constexpr int BLOCKS_PER_SM = 1;
 static_assert(BLOCKS_PER_SM * (WARPS_PER_BLOCK * sizeof(WarpSmem) + 1024) <= 228 * 1024,
               "WarpSmem too large for the blocks per SM");
 
@@ -26,10 +28,10 @@ __device__ __forceinline__ WarpSmem *warp_smem() {
 // one of the positions [k * num_sms, (k + 1) * num_sms), in the order the SMs
 // reach that level; every later job comes from the shared queue, and a claim
 // flag per position makes each job run exactly once. A giant job (marked by
-// the host, far above the average share) gets its SM to itself as far as the
-// schedule allows: the other warps of its block leave before taking a job,
-// and the SM's other warps take no new job while it runs. Their positions
-// and share of the queue go to the other SMs.
+// the host: one of the largest, far above the average share, at most one per
+// SM) takes three adjacent block-mates as helpers for its DP rows and their
+// shared memory as its ring; the block's other warps keep taking jobs, and
+// the helpers join them when the giant job is done.
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *sched, int num_sms, DevParams P, char *arenas,
             int64_t slot_bytes, int slots) {
@@ -43,13 +45,16 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   int32_t *queue = sched;
   int32_t *sm_count = sched + 4;
   int32_t *level_count = sm_count + SCHED_SM_SLOTS;
-  int32_t *sm_giant = level_count + SCHED_LEVELS;
-  int32_t *claim = sm_giant + SCHED_SM_SLOTS;
+  int32_t *claim = level_count + SCHED_LEVELS;
   unsigned smid = 0;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
   const bool sm_ok = smid < unsigned(SCHED_SM_SLOTS);
-  __shared__ int block_giant;
-  if (threadIdx.x == 0) block_giant = 0;
+  __shared__ int block_giant, giant_warp;
+  if (threadIdx.x == 0) {
+    block_giant = 0;
+    giant_warp = -1;
+  }
+  ring_default(sm);
   __syncthreads();
   int first = -1, first_giant = 0;
   if (active && lane == 0 && sm_ok) {
@@ -59,17 +64,47 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
       if (p0 < n_jobs) {
         first = int(p0);
         first_giant = jobs[order[p0]].giant;
-        if (first_giant) atomicOr(&block_giant, 1);
+        if (first_giant) {
+          atomicAdd(&block_giant, 1);
+          giant_warp = int(threadIdx.x >> 5);
+        }
       }
     }
   }
   __syncthreads();
-  if (!active) return;
+  // a giant gets three adjacent block-mates as helpers for its DP rows
+  // (cooperative rows) and their slices of shared memory as its ring (M,
+  // then D); every warp of the block sees the same block_giant and
+  // giant_warp. Warps past the last slot serve as helpers too: a helper
+  // needs no arena while it helps.
+  const int me = int(threadIdx.x >> 5);
+  const bool coop_block = block_giant == 1;
+  const int h0 = giant_warp + 3 < WARPS_PER_BLOCK ? giant_warp + 1 : giant_warp - 3;
+  if (coop_block && me >= h0 && me < h0 + 3) {
+    WarpSmem *leader = reinterpret_cast<WarpSmem *>(sm) - me + giant_warp;
+    coop_helper(reinterpret_cast<CoopDesc *>(leader->ring_m), me - h0 + 1);
+    // released: the slice is this warp's own again, and it takes jobs from
+    // the shared queue (its start position went to the queue)
+    if (!active) return;
+    ring_default(sm);
+    first = -1;
+    first_giant = 0;
+  } else if (!active) {
+    return;
+  }
   first = __shfl_sync(FULL, first, 0);
   first_giant = __shfl_sync(FULL, first_giant, 0);
-  // the other warps of a giant's block leave its SM share to it; the queue
-  // positions they would have started with go to the shared queue
-  if (block_giant && !first_giant) return;
+  if (first_giant && coop_block) {
+    WarpSmem *base = reinterpret_cast<WarpSmem *>(sm) - me + h0;
+    const int cap = int(3 * sizeof(WarpSmem) / 8 / 8 * 8);
+    if (lane == 0) {
+      sm->rv.m = reinterpret_cast<int32_t *>(base);
+      sm->rv.d = reinterpret_cast<int32_t *>(base) + cap;
+      sm->rv.cap = cap;
+      sm->rv.pad[0] = 1;  // cooperative rows for the first (giant) job
+    }
+    __syncwarp();
+  }
   if (lane == 0 && first >= 0 && atomicExch(&claim[first], 1) != 0) first = -1;
   first = __shfl_sync(FULL, first, 0);
   for (;;) {
@@ -77,20 +112,14 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     first = -1;
     if (q < 0) {
       if (lane == 0) {
-        if (sm_ok && atomicAdd(&sm_giant[smid], 0) != 0) {
-          q = n_jobs;  // this SM is running a giant job
-        } else {
-          do {
-            q = atomicAdd(queue, 1);
-          } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
-        }
+        do {
+          q = atomicAdd(queue, 1);
+        } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
       }
       q = __shfl_sync(FULL, q, 0);
       if (q >= n_jobs) break;
     }
     Job *J = jobs + order[q];
-    const bool giant = J->giant != 0 && sm_ok;
-    if (giant && lane == 0) atomicExch(&sm_giant[smid], 1);
     const int n_reads = J->n_reads;
     char *ja = J->arena ? J->arena : arena;
     const int64_t jb = J->arena ? J->arena_bytes : slot_bytes;
@@ -107,19 +136,24 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
         if (st == ST_OK) st = fs;
       }
       J->status = st;
-      if (giant) atomicExch(&sm_giant[smid], 0);
       if (J->done_flag) {
         __threadfence_system();  // the descriptor before the flag the host polls
         *reinterpret_cast<volatile int32_t *>(J->done_flag) = 1;
       }
     }
     __syncwarp();
+    // the giant job is done: the helpers go back to the queue
+    if (sm->rv.pad[0]) coop_release(sm);
   }
+  // no job at all (the first position was claimed elsewhere and the queue is
+  // empty): the helpers still wait for their release
+  if (sm->rv.pad[0]) coop_release(sm);
 }
 
 // Plain form: one launch aligns one read of one job.
 __global__ void k_extend_step(Job *J, DevParams P, char *arena, int64_t bytes, int r) {
   if (J->status != ST_OK || J->next_read != r) return;
+  ring_default(warp_smem());
   int32_t st = extend_one(J, P, arena, bytes, J->reads + J->read_off[r], J->read_len[r], r, warp_smem());
   if ((threadIdx.x & 31) == 0) {
     if ((st == ST_OK && r + 1 == J->n_reads) || is_alignment_error(st)) {
@@ -134,6 +168,7 @@ __global__ void k_extend_step(Job *J, DevParams P, char *arena, int64_t bytes, i
 __global__ void k_extend_range(Job *J, DevParams P, char *arena, int64_t bytes, const uint8_t *reads,
                                const int64_t *read_off, const int32_t *read_len, int r0, int r1) {
   int32_t st = ST_OK;
+  ring_default(warp_smem());
   for (int r = r0; r < r1; ++r) {
     st = extend_one(J, P, arena, bytes, reads + read_off[r], read_len[r], r, warp_smem());
     if (st != ST_OK) break;
@@ -157,6 +192,7 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
   int n_items = 0;
   Work cells{};
   int32_t st;
+  ring_default(warp_smem());
   if (mode == 0) {
     st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, warp_smem());
   } else if (retry) {
@@ -189,6 +225,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   const int lane = threadIdx.x & 31;
   const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   if (w >= n_win) return;
+  ring_default(warp_smem());
   const int4 d = win[w];  // (beg, end, qbeg, qlen | adaptive << 31)
   const bool adaptive = (unsigned(d.w) >> 31) != 0;
   const int qlen = d.w & 0x7fffffff;

@@ -86,6 +86,7 @@ __global__ void k_align_noalloc(Job *J, DevParams P, char *arena, int64_t bytes,
   Scratch s;
   int n_items = 0;
   Work cells{};
+  ring_default(noalloc_warp_smem());
   const int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, noalloc_warp_smem());
   if (st == ST_OK) {
     for (int k = lane; k < n_items; k += 32) {
