@@ -77,9 +77,9 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   // then D); every warp of the block sees the same block_giant and
   // giant_warp. Warps past the last slot serve as helpers too: a helper
   // needs no arena while it helps.
-  const int me = int(threadIdx.x >> 5);
-  const bool coop_block = block_giant == 1;
-  const int h0 = giant_warp + 3 < WARPS_PER_BLOCK ? giant_warp + 1 : giant_warp - 3;
+  const int me = int(threadIdx.x >> 5), wpb = int(blockDim.x >> 5);
+  const int h0 = giant_warp < 0 ? -1 : (giant_warp + 3 < wpb ? giant_warp + 1 : (giant_warp >= 3 ? giant_warp - 3 : -1));
+  const bool coop_block = block_giant == 1 && h0 >= 0;
   if (coop_block && me >= h0 && me < h0 + 3) {
     WarpSmem *leader = reinterpret_cast<WarpSmem *>(sm) - me + giant_warp;
     coop_helper(reinterpret_cast<CoopDesc *>(leader->ring_m), me - h0 + 1);
@@ -312,16 +312,20 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
 
 cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
                          const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
-  const int blocks = (slots + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-  const size_t smem = WARPS_PER_BLOCK * sizeof(WarpSmem);
+  // fewer slots than a full machine: narrower blocks, so that the warps
+  // spread over all SMs instead of filling a few
+  int wpb = WARPS_PER_BLOCK;
+  if (num_sms > 0 && slots < num_sms * WARPS_PER_BLOCK) wpb = std::max(1, (slots + num_sms - 1) / num_sms);
+  const int blocks = (slots + wpb - 1) / wpb;
   static bool attr = false;
   if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(WARPS_PER_BLOCK * sizeof(WarpSmem)));
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_batch<<<blocks, WARPS_PER_BLOCK * 32, smem, stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, sched,
-                                                          num_sms, P, arenas, slot_bytes, slots);
+  k_batch<<<blocks, wpb * 32, wpb * sizeof(WarpSmem), stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, sched,
+                                                                num_sms, P, arenas, slot_bytes, slots);
   return cudaGetLastError();
 }
 
@@ -349,16 +353,10 @@ cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t 
 cudaError_t launch_windows(Job *job_dev, const DevParams &P, char *arenas, int64_t slot_bytes, int n_win,
                            const int4 *win, const uint64_t *band, const uint8_t *query, int4 *items,
                            const int64_t *item_off, int32_t *out_n, int32_t *out_st, cudaStream_t stream) {
-  const size_t smem = WARPS_PER_BLOCK * sizeof(WarpSmem);
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  const int blocks = (n_win + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-  k_windows<<<blocks, WARPS_PER_BLOCK * 32, smem, stream>>>(job_dev, P, arenas, slot_bytes, n_win, win, band, query,
-                                                            items, item_off, out_n, out_st);
+  if (n_win <= 0) return cudaSuccess;
+  // one warp per block: the windows of a launch spread over all SMs
+  k_windows<<<n_win, 32, sizeof(WarpSmem), stream>>>(job_dev, P, arenas, slot_bytes, n_win, win, band, query, items,
+                                                     item_off, out_n, out_st);
   return cudaGetLastError();
 }
 
