@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   unsigned smid = 0;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
   const bool sm_ok = smid < unsigned(SCHED_SM_SLOTS);
-  __shared__ int block_giant, giant_warp;
+  __shared__ int block_giant, giant_warp, firsts[WARPS_PER_BLOCK];
   if (threadIdx.x == 0) {
     block_giant = 0;
     giant_warp = -1;
@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
       }
     }
   }
+  if (lane == 0) firsts[threadIdx.x >> 5] = first;
   __syncthreads();
   // a giant gets three adjacent block-mates as helpers for its DP rows
   // (cooperative rows) and their slices of shared memory as its ring (M,
@@ -78,10 +79,27 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   // giant_warp. Warps past the last slot serve as helpers too: a helper
   // needs no arena while it helps.
   const int me = int(threadIdx.x >> 5), wpb = int(blockDim.x >> 5);
-  const int h0 = giant_warp < 0 ? -1 : (giant_warp + 3 < wpb ? giant_warp + 1 : (giant_warp >= 3 ? giant_warp - 3 : -1));
+  int lead = giant_warp;
+  int h0 = giant_warp < 0 ? -1 : (giant_warp + 3 < wpb ? giant_warp + 1 : (giant_warp >= 3 ? giant_warp - 3 : -1));
+  if (block_giant == 1 && wpb == 8 && int64_t(blockIdx.x) * wpb + 4 < slots) {
+    // in a full 8-warp block the giant runs on warp 4 with warps 0-2 as
+    // helpers: warps map to the SM's four sub-partitions by index mod 4, so
+    // the giant shares its sub-partition with a helper, which is parked
+    // while the giant runs its band guides and traceback. Warp 4 and the
+    // giant's warp swap their first jobs.
+    lead = 4;
+    h0 = 0;
+    if (me == 4 && giant_warp != 4) {
+      first = firsts[giant_warp];
+      first_giant = 1;
+    } else if (me == giant_warp && giant_warp != 4) {
+      first = firsts[4];
+      first_giant = 0;
+    }
+  }
   const bool coop_block = block_giant == 1 && h0 >= 0;
   if (coop_block && me >= h0 && me < h0 + 3) {
-    WarpSmem *leader = reinterpret_cast<WarpSmem *>(sm) - me + giant_warp;
+    WarpSmem *leader = reinterpret_cast<WarpSmem *>(sm) - me + lead;
     coop_helper(reinterpret_cast<CoopDesc *>(leader->ring_m), me - h0 + 1);
     // released: the slice is this warp's own again, and it takes jobs from
     // the shared queue (its start position went to the queue)
