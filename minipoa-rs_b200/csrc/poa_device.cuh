@@ -1122,7 +1122,6 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
     const int ps = __shfl_sync(FULL, my_ps, t);
     const int pl = __shfl_sync(FULL, my_pl, t);
     const int pos = __shfl_sync(FULL, my_pos, t);
-    const int32_t *gp = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
     int4 m4[G], d4[G];
     int32_t prev[G];
     bool in[G];
@@ -1137,6 +1136,8 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
         prev[g] = rm[x == 0 ? cap - 1 : x - 1];
       }
     } else {
+      // the predecessor row has left the ring: its arena row
+      const int32_t *gp = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
 #pragma unroll
       for (int g = 0; g < G; ++g) {
         const int j0 = start + 128 * g + 4 * lane;
@@ -1183,6 +1184,7 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
   }
   // (lanes below the shuffle distance get their own value back, and
   // y + d*4E <= y because gap penalties are never positive)
+  int32_t T[G];  // the stripe's own insertion state leaving its last column
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     int32_t y = X[g][3];
@@ -1190,15 +1192,18 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
     for (int d = 1; d < 32; d <<= 1) y = __viaddmax_s32(__shfl_up_sync(FULL, y, d), d * 4 * E, y);
     pre[g] = __shfl_up_sync(FULL, y, 1);
     if (lane == 0) pre[g] = BELOW;
+    T[g] = __shfl_sync(FULL, y, 31);
   }
   // chain the stripes: carry = I at the stripe's first column (NEG32 at the
-  // band start); each lane's carried-in state is max(pre, carry shifted)
+  // band start), carry[g+1] = max(carry[g] + 128E, T[g]); each lane's
+  // carried-in state is max(pre, carry shifted). The T are independent, so
+  // the chain is arithmetic only.
   int32_t cin[G];
   int32_t carry = NEG32;
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     cin[g] = __viaddmax_s32(carry, 4 * lane * E, pre[g]);
-    if (g + 1 < G) carry = __shfl_sync(FULL, __viaddmax_s32(cin[g], 4 * E, X[g][3]), 31);
+    if (g + 1 < G) carry = __viaddmax_s32(carry, 128 * E, T[g]);
   }
   __syncwarp();  // every predecessor read of the ring precedes this row's writes
 #pragma unroll

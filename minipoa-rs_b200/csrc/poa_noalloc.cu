@@ -104,7 +104,8 @@ __global__ void k_align_noalloc(Job *J, DevParams P, char *arena, int64_t bytes,
 // graph of n rows and e edges and a query of qlen bases.
 int64_t scratch_floor(int64_t n, int64_t e, int64_t qlen) {
   const int64_t padded = (qlen + 2) / 8 * 8 + 8;
-  return n * (12 * 8 + 7 * 4) + (e + 1) * (8 + 8 + 16 + 8) + (padded + 32) * 5 + (qlen + 4) * 16 + 33 * 128;
+  return n * (12 * 8 + 8 * 4 + 2 * 16) + (e + 1) * (8 + 8 + 16 + 8 + 16) + (padded + 32) * 5 + (qlen + 4) * 16 +
+         34 * 128;
 }
 
 }  // namespace
