@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=1003)
     ap.add_argument("--lmax", type=int, default=5000, help="largest ancestor length (smaller for profiling runs)")
     ap.add_argument("--dmax", type=int, default=60, help="largest read depth (smaller for profiling runs)")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-sets", type=int, default=64, help="sets timed in the plain per-read form")
     ap.add_argument("--mem-budget-gb", type=float, default=0.0,
@@ -158,31 +158,86 @@ def barrier(pg):
         pg.barrier()
 
 
-def cpu_baseline(sets, params, seconds: float):
-    """Oracle AVX2 kernel on all host threads over a bounded sample of the
-    same sets (taken in set order until about `seconds` of CPU time)."""
+def set_work(reads, params) -> float:
+    """Estimated band cells of one read set (for sampling): reads x rows x band."""
+    if not reads:
+        return 0.0
+    L = max(len(r) for r in reads)
+    w = min(2.0 * (params.b + (L / params.f if params.f else L)) + 16.0, L + 16.0)
+    return sum(len(r) for r in reads) * w * (1.0 + 0.03 * len(reads))
+
+
+def cpu_sample(sets, params, seconds: float, threads: int, rate_per_thread: float = 0.12e9):
+    """A fixed, size-stratified sample of the sets for the CPU leg: the 8
+    largest sets, then every k-th set of the size-ordered list, with k chosen
+    so the estimated work is about `seconds` on `threads` threads at
+    `rate_per_thread` cells/s. Returned largest first, so the oracle's atomic
+    queue keeps every thread busy until the end."""
+    order = sorted(range(len(sets)), key=lambda s: -set_work(sets[s], params))
+    budget = seconds * threads * rate_per_thread
+    total = sum(set_work(sets[s], params) for s in order)
+    k = max(1, int(total / max(1.0, budget)))
+    pick = order[:8] + order[8::k]
+    out, acc = [], 0.0
+    for s in pick:
+        if acc > budget and len(out) >= 8:
+            break
+        out.append(s)
+        acc += set_work(sets[s], params)
+    return out
+
+
+def cpu_baseline(sets, params, seconds: float, threads: int = 0):
+    """The oracle's 8-lane AVX2 i32 kernel over a fixed sample of the same
+    sets (cpu_sample) in ONE call on `threads` host threads (default: all),
+    largest set first, so the atomic work queue keeps every thread busy.
+    Returns the measurement plus the sample's consensus hashes."""
     import oracle
 
-    threads = os.cpu_count() or 1
-    done_cells, done_sets, elapsed = 0, 0, 0.0
-    chunk = max(threads, 8)
-    i = 0
-    while i < len(sets) and elapsed < seconds:
-        part = sets[i:i + chunk]
-        t0 = time.perf_counter()
-        cells, _ = oracle.batch_run(params, part, kernel=oracle.AUTO_AVX2, threads=threads, out_format=0)
-        elapsed += time.perf_counter() - t0
-        done_cells += cells
-        done_sets += len(part)
-        i += chunk
+    threads = threads or os.cpu_count() or 1
+    sample = cpu_sample(sets, params, seconds, threads)
+    part = [sets[s] for s in sample]
+    t0 = time.perf_counter()
+    cells, hashes = oracle.batch_run(params, part, kernel=oracle.AUTO_AVX2, threads=threads, out_format=0)
+    elapsed = time.perf_counter() - t0
     return {
-        "value": done_cells / elapsed / 1e9 if elapsed > 0 else None,
+        "value": cells / elapsed / 1e9 if elapsed > 0 else None,
         "unit": "GCUPS",
         "cores": threads,
         "kind": "port",
-        "sample": f"first {done_sets} of the {len(sets)} sets ({done_cells / 1e9:.2f} G cells, {elapsed:.1f} s), "
-                  f"8-lane AVX2 i32 kernel, one set per thread",
-    }
+        "sample": f"{len(sample)} of the {len(sets)} sets (the 8 largest, then every k-th by size; "
+                  f"{cells / 1e9:.2f} G cells, {elapsed:.1f} s), 8-lane AVX2 i32 kernel, one call, "
+                  f"largest first over {threads} threads",
+    }, dict(zip(sample, hashes))
+
+
+def cpu_single_thread(sets, params, seconds: float):
+    """The same kernel on one thread over a small stratified sample (the
+    reference's unseeded runs are single-threaded whatever -t is)."""
+    import oracle
+
+    order = sorted(range(len(sets)), key=lambda s: -set_work(sets[s], params))
+    budget = seconds * 0.12e9
+    total = sum(set_work(sets[s], params) for s in order)
+    k = max(1, int(total / budget))
+    sample = order[k // 2::k] or order[-1:]
+    t0 = time.perf_counter()
+    cells, _ = oracle.batch_run(params, [sets[s] for s in sample], kernel=oracle.AUTO_AVX2, threads=1, out_format=-1)
+    dt = time.perf_counter() - t0
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": 1,
+            "sample": f"{len(sample)} sets, every k-th by size ({cells / 1e9:.2f} G cells, {dt:.1f} s)"}
+
+
+def consensus_parity(gpu_text: bytes, hashes: dict):
+    """Compares the GPU's consensus of the sampled sets (from the all-sets
+    output, split per set) with the oracle's hashes of the same sets."""
+    import oracle
+
+    head = b">consensus sequence\n"
+    parts = gpu_text.split(head)[1:]
+    bad = [s for s, h in hashes.items() if s >= len(parts) or oracle.fnv1a(head + parts[s]) != h]
+    return {"sets_checked": len(hashes), "mismatches": len(bad), "output": "consensus FASTA bytes (FNV-1a)",
+            "mismatched_sets": bad[:16]}
 
 
 def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006):
@@ -306,7 +361,7 @@ def main():
         t_steps = []
         cb = None
         for k in range(args.warmup + args.steps):
-            cb = cpu_baseline(sets, params, max(2.0, args.cpu_seconds / max(1, args.steps)))
+            cb, _ = cpu_baseline(sets, params, max(2.0, args.cpu_seconds / max(1, args.steps)))
             if k >= args.warmup:
                 t_steps.append(cb)
         vals = [c["value"] for c in t_steps]
@@ -356,6 +411,7 @@ def main():
 
     # end to end through the C ABI from host buffers
     e2e_vals, h2d, d2h = [], 0, 0
+    out = None
     for _ in range(0 if args.no_e2e else max(1, min(args.steps, 2))):
         t0 = time.perf_counter()
         b2 = mp.Batch(params, sets, ctx)
@@ -410,9 +466,33 @@ def main():
         except Exception as e:
             seeded = {"error": str(e)}
 
-    cb = None
+    cb, parity = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        cb = cpu_baseline(sets, params, args.cpu_seconds)
+        cb, hashes = cpu_baseline(sets, params, args.cpu_seconds)
+        cb["single_thread"] = cpu_single_thread(sets, params, max(3.0, args.cpu_seconds / 3))
+        if out is not None:
+            parity = consensus_parity(out, hashes)
+            print(f"[bench] parity: {parity['sets_checked']} sets checked, {parity['mismatches']} mismatches",
+                  file=sys.stderr, flush=True)
+
+    # integer-ALU roofline: (6 + 5 P) adds and maxes per cell, P the in-band
+    # predecessors (counted as predecessor-cell updates), against the measured
+    # integer throughput of this GPU
+    int_roof = None
+    try:
+        peaks = mp.int_peak(local)
+        int_peak = max(peaks)
+        pred_cells = sum(s.pred_cells for s in steps)
+        ops = 6.0 * cells + 5.0 * pred_cells
+        ach = ops / (kern_ms / 1e3)
+        int_roof = {"bound": "int32 ALU", "achieved": ach / 1e12, "peak": int_peak / 1e12, "unit": "Tops/s",
+                    "frac": ach / int_peak, "ops_per_cell": ops / max(1, cells),
+                    "preds_per_cell": pred_cells / max(1, cells),
+                    "peak_source": "measured on this GPU (poa_probe_int_peak): add, max, fused add-max = "
+                                   + ", ".join(f"{x / 1e12:.1f}" for x in peaks) + " Tops/s; the largest is the peak",
+                    "kernel": "k_batch"}
+    except Exception as e:
+        int_roof = {"error": str(e)}
 
     if rank == 0:
         line = {
@@ -423,8 +503,13 @@ def main():
                        "sets": args.sets, "seed": args.seed, "reads_per_step": reads // args.steps,
                        "cells_per_step": cells // args.steps, "l2": "inputs larger than L2 (no flush needed)",
                        "parallelism": f"{world} independent GPU(s)", "slots": first_slots,
-                       "relaunch_passes": first_passes, "reads_per_s": reads / (dev_ms / 1e3)},
+                       "relaunch_passes": first_passes, "reads_per_s": reads / (dev_ms / 1e3),
+                       "paths": {"giant_jobs_with_helpers": steps[0].coop_jobs, "rows_4_stripe": steps[0].rows_g4,
+                                 "rows_generic": steps[0].rows_generic,
+                                 "pred_rows_from_arena": steps[0].far_preds}},
             "roofline": roofline,
+            "roofline_int": int_roof,
+            "parity": parity,
             "cpu_baseline": cb,
             "e2e": {"value": e2e_v, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

@@ -234,6 +234,13 @@ typedef struct poa_batch_stats {
   int32_t reserved;
   double kernel_ms;     /* device time inside the read-loop kernel launches */
   uint64_t dp_bytes;    /* DP state bytes stored (M, D, I per cell) */
+  uint64_t pred_cells;  /* predecessor-cell updates: per row, the band overlap of each
+                           in-band predecessor (align.rs:751-797 trip count) */
+  uint64_t far_preds;   /* predecessor rows read from the arena, not the shared-memory ring */
+  uint64_t rows_g4;     /* DP rows of the 4-stripe tile (385-512 columns) */
+  uint64_t rows_generic;  /* DP rows of the generic row (wider, > 32 predecessors, i64) */
+  int32_t coop_jobs;    /* jobs that ran cooperative rows (a giant with helper warps) */
+  int32_t reserved2;
 } poa_batch_stats;
 
 /* Uploads n_sets read sets (set i = reads set_off[i]..set_off[i+1]-1) and
@@ -260,6 +267,13 @@ int poa_batch_graph(poa_ctx *ctx, poa_batch *batch, int64_t set, poa_graph **out
  * lengths) and by the last output call (packed graphs). */
 int poa_batch_transfer_bytes(poa_ctx *ctx, poa_batch *batch, uint64_t *h2d, uint64_t *d2h);
 void poa_batch_free(poa_batch *batch);
+
+/* Integer-pipe throughput of `device` (no reference counterpart: the
+ * roofline denominator of the DP kernels, whose recurrences are 32-bit adds
+ * and maxes). Fills out_ops_per_s[3] with operations per second of a plain
+ * add, a plain max and the DPX fused add-max (two operations each), each
+ * over every SM. Allocates a small device buffer; about 0.1 s. */
+int poa_probe_int_peak(int32_t device, double *out_ops_per_s);
 
 /* Tuning: concurrent warp slots per SM for the batched kernel (0 = auto) and
  * the DP arena bytes per slot (0 = auto from the budget). */

@@ -104,12 +104,21 @@ struct Job {
   int32_t *done_flag;   // when set (host-mapped memory), raised once the job leaves the kernel
   uint64_t cells;       // DP cells of completed reads (retries included)
   uint64_t dp_bytes;    // DP state bytes stored for those cells (M, D, I)
+  uint64_t pred_cells;  // predecessor-cell updates of those reads (band overlaps)
+  uint64_t far_preds;   // predecessor rows read from the arena (left the ring)
+  uint64_t rows_g4;     // rows of the 4-stripe tile (385-512 columns)
+  uint64_t rows_generic;  // rows of the generic row (wider bands, many predecessors, i64)
+  int32_t coop;         // 1 once a read of the job ran cooperative rows
+  int32_t reserved2;
 };
 
-// Work counted by one alignment: 8-aligned band cells and the bytes of DP
-// state they stored.
+// Work counted by one alignment: 8-aligned band cells, the bytes of DP
+// state they stored, the predecessor-cell updates (the sum over rows of each
+// in-band predecessor's band overlap, the reference's predecessor loop
+// trip count) and which row paths ran.
 struct Work {
-  uint64_t cells, dp_bytes;
+  uint64_t cells, dp_bytes, pred_cells, far_preds, rows_g4, rows_generic;
+  int32_t coop;
 };
 
 // Per-read scratch carved from the front of a warp slot's arena.
@@ -1499,15 +1508,20 @@ __device__ __forceinline__ int4 ld_early(const int4 *p) {
 // RING_CAP entries were written since), else -1, plus its arena offset. A row
 // goes through the ring when `ring` is set, its band is at most RING_MAX_LEN
 // and it has at most 32 predecessors (row 0: when its band fits).
-__device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap) {
+__device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w) {
   const int lane = threadIdx.x & 31;
   int carry = 0;  // rows before this block that did not go through the ring
+  uint64_t g4 = 0, gen = 0, far = 0;
   for (int i0 = 0; i0 < n; i0 += 32) {
     const int i = i0 + lane;
     bool fast = true;
     if (i < n) {
       const int len = s.row_len[i], pc = s.pred_cnt[i];
       fast = ring && len <= RING_MAX_LEN && (i == 0 || pc <= 32);
+      if (i > 0 && len > 0) {
+        g4 += fast && len > 384 ? 1 : 0;
+        gen += fast ? 0 : 1;
+      }
       const int64_t off = s.row_off[i];
       s.plan[i] = make_int4(s.row_start[i], len, s.pred_start[i], pc);
       s.plan2[i] = make_int4(int(uint64_t(off) & 0xffffffffu), int(uint64_t(off) >> 32), s.row_base[i],
@@ -1526,10 +1540,40 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap) {
       const int64_t po = s.pmeta_off[pb + t];
       int pos = -1;
       if (m.x >= 0 && m.z > 0 && s.nf[m.x] == nfi && off - po <= 3 * int64_t(cap)) pos = int((po / 3) % cap);
+      if (m.x >= 0 && m.z > 0 && pos < 0 && s.row_len[i] > 0 && s.row_len[i] <= RING_MAX_LEN) ++far;
       s.pmeta2[pb + t] = make_int4(pos, int(uint64_t(po) & 0xffffffffu), int(uint64_t(po) >> 32), 0);
     }
   }
   __syncwarp();
+  for (int d = 16; d; d >>= 1) {
+    g4 += __shfl_xor_sync(FULL, g4, d);
+    gen += __shfl_xor_sync(FULL, gen, d);
+    far += __shfl_xor_sync(FULL, far, d);
+  }
+  w->rows_g4 += g4;
+  w->rows_generic += gen;
+  w->far_preds += far;
+}
+
+// Predecessor-cell updates of a planned read (after fill_pmeta): the sum
+// over rows of each in-band predecessor's band overlap, which is the trip
+// count of the reference's predecessor loop (align.rs:751-797).
+__device__ inline uint64_t pred_overlap_cells(const Scratch &s, int n) {
+  const int lane = threadIdx.x & 31;
+  uint64_t tot = 0;
+  for (int i = 1 + lane; i < n; i += 32) {
+    const int rs = s.row_start[i], rl = s.row_len[i];
+    if (rl <= 0) continue;
+    const int pb = s.pred_start[i], pc = s.pred_cnt[i];
+    for (int t = 0; t < pc; ++t) {
+      const int4 m = s.pmeta[pb + t];
+      if (m.x < 0 || m.z <= 0) continue;
+      const int lo = max(rs, m.y), hi = min(rs + rl, m.y + m.z);
+      if (hi > lo) tot += uint64_t(hi - lo);
+    }
+  }
+  for (int d = 16; d; d >>= 1) tot += __shfl_xor_sync(FULL, tot, d);
+  return tot;
 }
 
 // Per predecessor entry: (row, band start, band length, edge weight) and the
@@ -1676,13 +1720,15 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     __syncwarp();
     fill_pmeta(s, n);
     const bool ring = kFastType && sm;
-    plan_rows(s, n, ring, rcap);
+    plan_rows(s, n, ring, rcap, cells);
+    cells->pred_cells += pred_overlap_cells(s, n);
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
     __syncwarp();
     if (ring) ring_put_row0(rm, rd, A, s.row_len[0]);
     // a lone giant's block-mates join the row loop (cooperative rows)
     const bool coop = ring && sm->rv.pad[0] != 0;
     CoopDesc *cd = coop ? reinterpret_cast<CoopDesc *>(sm->ring_m) : nullptr;
+    if (coop) cells->coop = 1;
     if (coop) {
       if (lane == 0) {
         cd->mode = COOP_ROWS;
@@ -1822,6 +1868,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
       S bestv = ScoreTraits<S>::LOWEST;
       int bestj = INT32_MAX;
       if (kFastType && sm && len <= RING_MAX_LEN && pc <= 32) {
+        if (len > 384) cells->rows_g4 += 1;
         int my_ps = 0, my_pl = 0, my_pos = -1;
         const int32_t *my_g = nullptr;
         bool ok = false;
@@ -1837,6 +1884,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
           }
         }
         const unsigned vmask = __ballot_sync(FULL, ok);
+        cells->far_preds += __popc(__ballot_sync(FULL, ok && my_pos < 0));
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
@@ -1846,6 +1894,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         bestj = bj;
       } else {
         ring_floor = off + 1;  // this row does not enter the ring
+        cells->rows_generic += 1;
         dp_row_generic<S>(lane, start, len, R, A, s, pb, pc, P.matrix + base * P.sigma, E, O, true, bestv, bestj);
       }
       __syncwarp();
@@ -1869,6 +1918,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   if (do_adapt) {
     __syncwarp();
     fill_pmeta(s, n);
+    cells->pred_cells += pred_overlap_cells(s, n);
   }
   st = traceback<S>(J, P, s, A, beg, n, m, (sm && smem_matrix) ? sm->matrix : P.matrix, n_items);
   return st;
@@ -2180,6 +2230,11 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
     if (st == ST_OK) {
       J->cells += cells.cells;
       J->dp_bytes += cells.dp_bytes;
+      J->pred_cells += cells.pred_cells;
+      J->far_preds += cells.far_preds;
+      J->rows_g4 += cells.rows_g4;
+      J->rows_generic += cells.rows_generic;
+      J->coop |= cells.coop;
       J->next_read = r + 1;
     }
   }

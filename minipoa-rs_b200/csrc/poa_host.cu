@@ -1320,14 +1320,26 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
     b->download_jobs();
     b->ran = true;
     if (stats) {
-      uint64_t cells = 0, reads = 0, dpb = 0;
+      uint64_t cells = 0, reads = 0, dpb = 0, pc = 0, far = 0, g4 = 0, gen = 0;
+      int32_t coop = 0;
       for (auto &J : b->jobs) {
         cells += J.cells;
         dpb += J.dp_bytes;
         reads += uint64_t(J.next_read);
+        pc += J.pred_cells;
+        far += J.far_preds;
+        g4 += J.rows_g4;
+        gen += J.rows_generic;
+        coop += J.coop;
       }
       stats->cells = cells;
       stats->dp_bytes = dpb;
+      stats->pred_cells = pc;
+      stats->far_preds = far;
+      stats->rows_g4 = g4;
+      stats->rows_generic = gen;
+      stats->coop_jobs = coop;
+      stats->reserved2 = 0;
       stats->kernel_ms = kernel_ms;
       stats->reads = reads;
       stats->device_ms = ms;

@@ -325,6 +325,11 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   J->n_items = 0;
   J->cells = 0;
   J->dp_bytes = 0;
+  J->pred_cells = 0;
+  J->far_preds = 0;
+  J->rows_g4 = 0;
+  J->rows_generic = 0;
+  J->coop = 0;
   J->order_exact = 1;
 }
 

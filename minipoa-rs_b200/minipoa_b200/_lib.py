@@ -52,7 +52,9 @@ POA_SERVER_QUEUED, POA_SERVER_RUNNING, POA_SERVER_DONE, POA_SERVER_FAILED, POA_S
 class BatchStats(ctypes.Structure):
     _fields_ = [("cells", ctypes.c_uint64), ("reads", ctypes.c_uint64), ("device_ms", ctypes.c_double),
                 ("launches", ctypes.c_int32), ("relaunches", ctypes.c_int32), ("slots", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("kernel_ms", ctypes.c_double), ("dp_bytes", ctypes.c_uint64)]
+                ("reserved", ctypes.c_int32), ("kernel_ms", ctypes.c_double), ("dp_bytes", ctypes.c_uint64),
+                ("pred_cells", ctypes.c_uint64), ("far_preds", ctypes.c_uint64), ("rows_g4", ctypes.c_uint64),
+                ("rows_generic", ctypes.c_uint64), ("coop_jobs", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes); every function declared in include/minipoa_b200.h
@@ -97,6 +99,7 @@ SIGNATURES = {
     "poa_batch_graph": (ctypes.c_int, [_vp, _vp, _i64, P(_vp)]),
     "poa_batch_free": (None, [_vp]),
     "poa_batch_tune": (ctypes.c_int, [_vp, _vp, _i32, _u64]),
+    "poa_probe_int_peak": (ctypes.c_int, [_i32, P(ctypes.c_double)]),
     "poa_align_noalloc": (ctypes.c_int, [_vp, _cp, _vp, _vp, _i64, _vp, _i64, _vp]),
     "poa_batch_transfer_bytes": (ctypes.c_int, [_vp, _vp, P(_u64), P(_u64)]),
     "poa_server_create": (ctypes.c_int, [_vp, _cp, _u64, _i32, P(_vp)]),

@@ -25,6 +25,16 @@ def dp_backend() -> str:
     return _lib.load().poa_dp_backend().decode()
 
 
+def int_peak(device: int = 0) -> Tuple[float, float, float]:
+    """Measured integer-pipe throughput of `device` in operations per second:
+    (plain add, plain max, fused add-max counted as two operations)."""
+    out = (ctypes.c_double * 3)()
+    rc = _lib.load().poa_probe_int_peak(device, out)
+    if rc != 0:
+        raise PoaError(rc, "integer throughput probe failed")
+    return out[0], out[1], out[2]
+
+
 def _bytes(x) -> bytes:
     return x.encode() if isinstance(x, str) else bytes(x)
 

@@ -100,6 +100,8 @@ def lib():
                                     ctypes.c_int, P(u64), P(u64)]
         L.orc_avx2_prefix.argtypes = [P(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                       P(ctypes.c_int32)]
+        L.orc_fnv1a.argtypes = [ctypes.c_char_p, i64]
+        L.orc_fnv1a.restype = u64
         _lib = L
     return _lib
 
@@ -351,3 +353,9 @@ def avx2_prefix(md: List[int], carry: int, open_: int, ext: int) -> List[int]:
 
 def avx2_available() -> bool:
     return bool(lib().orc_avx2_available())
+
+
+def fnv1a(data) -> int:
+    """FNV-1a of a text or byte string, the hash batch_run reports per set."""
+    b = data.encode() if isinstance(data, str) else bytes(data)
+    return lib().orc_fnv1a(b, len(b))

@@ -1337,6 +1337,12 @@ int orc_batch_run(const orc_params *p, int64_t n_sets, const int64_t *set_off, c
 
 int orc_avx2_available(void) { return __builtin_cpu_supports("avx2") ? 1 : 0; }
 
+// FNV-1a of a byte string: the hash orc_batch_run reports per set, so a
+// caller can compare another implementation's output text with it.
+uint64_t orc_fnv1a(const uint8_t *data, int64_t len) {
+  return fnv1a(std::string(reinterpret_cast<const char *>(data), size_t(len)));
+}
+
 __attribute__((target("avx2"))) void orc_avx2_prefix(const int32_t *md8, int32_t carry, int32_t open, int32_t ext,
                                                      int32_t *out8) {
   __m256i v = insertion_prefix(_mm256_loadu_si256((const __m256i *)md8), carry, open, ext);

@@ -1,0 +1,147 @@
+"""GPU parity on the code paths the benchmark times, against the CPU oracle.
+
+The batched benchmark launches thousands of read sets, so every block of the
+persistent kernel has its full eight warps and the largest sets run as
+"giants" with three helper warps computing their DP rows (cooperative rows).
+Sets of 3.6 kbp and more have bands of 385-512 columns (the 4-stripe row
+tile), and high-error sets have predecessor rows that left the shared-memory
+ring. A small batch reaches none of these, so these tests build batches that
+do, assert from the run's counters that each path ran, and compare every
+set's output with the oracle.
+
+Also here: protein families with full DP (-f0, bands wider than 512 columns:
+the generic row) and an i64 set whose reads are longer than the query bytes
+kept in shared memory.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import refcases as rc
+from minipoa_b200.params import Params, Sequence
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+
+
+@pytest.fixture(scope="module")
+def mp():
+    import minipoa_b200 as m
+
+    m.default_context()
+    return m
+
+
+def _full_machine_sets(seed, n_giants, giant_len, giant_depth, n_small):
+    """n_giants large high-error sets first, then many small ones, so that a
+    launch has one slot per warp of every SM and the giants are marked."""
+    rng = np.random.default_rng(seed)
+    sets = []
+    for g in range(n_giants):
+        e = 0.08 + 0.02 * g
+        sets.append(rc.synthetic_reads(rng, giant_len + 150 * g, giant_depth, 0.6 * e, 0.2 * e, 0.2 * e))
+    for _ in range(n_small):
+        L = int(rng.integers(40, 140))
+        e = rng.uniform(0.02, 0.15)
+        sets.append(rc.synthetic_reads(rng, L, int(rng.integers(3, 7)), 0.6 * e, 0.2 * e, 0.2 * e))
+    return sets
+
+
+def _gfa_hashes_match(oracle, batch, params, sets):
+    _, want = oracle.batch_run(params, sets, kernel=oracle.AUTO_AVX2, threads=THREADS, out_format=2)
+    bad = [s for s in range(len(sets)) if oracle.fnv1a(batch.output(s, 2)) != want[s]]
+    return bad
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive):
+    params = Params(adaptive=adaptive)
+    sets = _full_machine_sets(2024 + int(adaptive), 4, 4200, 30, 1180)
+    batch = mp.Batch(params, sets)
+    st = batch.run(0)
+    # one slot per resident warp of every SM in the first pass: full 8-warp
+    # blocks (an adaptive giant may outgrow its arena and finish in a second
+    # pass, which the comparison below covers too)
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert st.slots == min(len(sets), sms * 8)
+    assert st.rows_g4 > 0, "no 4-stripe rows ran"
+    assert st.far_preds > 0, "no predecessor row was read back from the arena"
+    if not adaptive:
+        assert st.coop_jobs >= 1, "no giant ran cooperative rows"
+    for s in range(len(sets)):
+        assert batch.status(s) is None
+    # every set: GFA bytes (graph, edges in order, paths) against the oracle
+    assert _gfa_hashes_match(oracle, batch, params, sets) == []
+    # the giants and a sample of small sets: whole graphs and MSA bytes
+    rng = np.random.default_rng(7)
+    sample = list(range(4)) + sorted(rng.choice(np.arange(4, len(sets)), 12, replace=False).tolist())
+    for s in sample:
+        reads = sets[s]
+        o = oracle.align_sequences(params, reads, kernel=oracle.AUTO_AVX2)
+        recs = [Sequence(name=f"read{i}", seq=x) for i, x in enumerate(reads)]
+        assert batch.graph(s).dump() == o.dump(5), f"set {s}"
+        assert batch.output(s, 0) == ">consensus sequence\n" + o.consensus(params)[0].decode() + "\n"
+        assert batch.output(s, 1, recs) == o.msa(params, recs)
+    # consensus of every set through the all-sets call
+    allc = batch.output_all(0).decode()
+    _, want0 = oracle.batch_run(params, sets, kernel=oracle.AUTO_AVX2, threads=THREADS, out_format=0)
+    parts = allc.split(">consensus sequence\n")[1:]
+    assert len(parts) == len(sets)
+    assert [oracle.fnv1a(">consensus sequence\n" + p) for p in parts] == want0
+
+
+def test_protein_families_full_dp_wide_rows_match_oracle(mp, oracle):
+    # 20-letter alphabet, symmetric matrix (diagonal 4..11, off-diagonal
+    # -4..2), -f0: every row spans the whole query (600-800 columns)
+    rng = np.random.default_rng(1004)
+    alpha = b"ACDEFGHIKLMNPQRSTVWYX"
+    k = len(alpha)
+    m = [0] * (k * k)
+    for i in range(k - 1):
+        for j in range(i, k - 1):
+            v = int(rng.integers(4, 12)) if i == j else int(rng.integers(-4, 3))
+            m[i * k + j] = m[j * k + i] = v
+    m[k * k - 1] = 5
+    params = Params(alphabet=alpha, matrix=m, f=0)
+    fams = []
+    for L in (640, 780):
+        anc = rng.integers(0, 20, size=L)
+        fam = []
+        for _ in range(30):
+            s = []
+            for a in anc:
+                u = rng.random()
+                if u < 0.025:
+                    continue  # deletion
+                s.append(int(rng.integers(0, 20)) if rng.random() < 0.15 else int(a))
+                if rng.random() < 0.025:
+                    s.append(int(rng.integers(0, 20)))  # insertion
+            fam.append(bytes(alpha[x] for x in s))
+        fams.append(fam)
+    batch = mp.Batch(params, fams)
+    st = batch.run(0)
+    assert st.rows_generic > 0, "no generic (wide) rows ran"
+    for f, reads in enumerate(fams):
+        o = oracle.align_sequences(params, reads, kernel=oracle.AUTO_AVX2)
+        assert batch.graph(f).dump() == o.dump(k)
+        recs = [Sequence(name=f"read{i}", seq=x) for i, x in enumerate(reads)]
+        assert batch.output(f, 1, recs) == o.msa(params, recs)
+
+
+def test_i64_reads_longer_than_shared_query_match_oracle(mp, oracle):
+    # match 10,000: the score guard selects the i64 kernel; 6 kbp reads do not
+    # fit the shared-memory query bytes, so the query is read from the arena
+    params = Params.from_cli_scores(match=10000)
+    reads = rc.synthetic_reads(np.random.default_rng(1005), 6000, 3, 0.01, 0.005, 0.005)
+    o = oracle.align_sequences(params, reads)
+    assert not o.i32_scores_safe(params, 0, 1, len(reads[-1]))
+    g = mp.align_sequences(params, reads)
+    assert g.dump() == o.dump(5)
+    batch = mp.Batch(params, [reads])
+    st = batch.run(0)
+    assert st.rows_generic > 0
+    assert batch.graph(0).dump() == o.dump(5)
