@@ -241,6 +241,8 @@ typedef struct poa_batch_stats {
   uint64_t rows_generic;  /* DP rows of the generic row (wider, > 32 predecessors, i64) */
   int32_t coop_jobs;    /* jobs that ran cooperative rows (a giant with helper warps) */
   int32_t reserved2;
+  uint64_t phase_cycles[4]; /* profiling builds only (POA_PHASE_CYCLES), else 0: warp cycles
+                               in band guides, DP rows, traceback, graph update */
 } poa_batch_stats;
 
 /* Uploads n_sets read sets (set i = reads set_off[i]..set_off[i+1]-1) and

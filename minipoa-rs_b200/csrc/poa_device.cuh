@@ -110,6 +110,8 @@ struct Job {
   uint64_t rows_generic;  // rows of the generic row (wider bands, many predecessors, i64)
   int32_t coop;         // 1 once a read of the job ran cooperative rows
   int32_t reserved2;
+  uint64_t phase[4];    // profiling builds (POA_PHASE_CYCLES): warp cycles in band guides,
+                        // DP rows, traceback, graph update (add_path + rank order)
 };
 
 // Work counted by one alignment: 8-aligned band cells, the bytes of DP
@@ -119,7 +121,16 @@ struct Job {
 struct Work {
   uint64_t cells, dp_bytes, pred_cells, far_preds, rows_g4, rows_generic;
   int32_t coop;
+  uint64_t phase[4];
 };
+
+// Warp cycle counters of the read loop's phases, compiled in for profiling
+// builds only (-DPOA_PHASE_CYCLES); otherwise the reads are constant zero.
+#ifdef POA_PHASE_CYCLES
+__device__ __forceinline__ uint64_t phase_clock() { return clock64(); }
+#else
+__device__ __forceinline__ uint64_t phase_clock() { return 0; }
+#endif
 
 // Per-read scratch carved from the front of a warp slot's arena.
 struct Scratch {
@@ -131,9 +142,9 @@ struct Scratch {
   int32_t *row_base;   // base code a row scores with (N for the last row)
   int4 *pmeta;         // per pred entry: (row, band start, band length, -)
   int64_t *pmeta_off;  // per pred entry: the predecessor row's arena offset
-  int4 *plan;          // static band, per row: (band start, band length, pred_start, pred_cnt)
-  int4 *plan2;         // static band, per row: (arena offset lo, hi, base code, ring entry)
-  int4 *pmeta2;        // static band, per pred entry: (ring entry or -1, arena offset lo, hi, -)
+  int4 *tb;            // traceback, two per pred entry: the predecessor row's descriptor (see fill_tb)
+  int4 *planc;         // static band, per row: (band start, band length, pred_start, pred_cnt | base << 24)
+  int4 *pent;          // static band, per pred entry: where the predecessor's states are (see plan_rows)
   int32_t *nf;         // static band, per row: rows before it that did not go through the ring
   int32_t *seq;        // encoded, padded query
   uint8_t *seq8;       // the same, one byte per column (when it does not fit shared memory)
@@ -178,9 +189,9 @@ __device__ inline bool carve_scratch(char *arena, int64_t bytes, int n, int e, i
   s.row_base = (int32_t *)take(N * 4);
   s.pmeta = (int4 *)take(int64_t(e + 1) * 16);
   s.pmeta_off = (int64_t *)take(int64_t(e + 1) * 8);
-  s.plan = (int4 *)take(N * 16);
-  s.plan2 = (int4 *)take(N * 16);
-  s.pmeta2 = (int4 *)take(int64_t(e + 1) * 16);
+  s.tb = (int4 *)take(int64_t(e + 1) * 32);
+  s.planc = (int4 *)take(N * 16);
+  s.pent = (int4 *)take(int64_t(e + 1) * 16);
   s.nf = (int32_t *)take(N * 4);
   s.seq = (int32_t *)take((padded + 32) * 4);
   s.seq8 = (uint8_t *)take(padded + 32);
@@ -832,37 +843,80 @@ __device__ inline void adaptive_update(const Job *J, Scratch &s, int beg, int i,
   }
 }
 
+// Per predecessor entry of every row, the descriptor a traceback step needs
+// to move to that predecessor (warp-wide, after the DP): tb[2e] = (row, band
+// start, band length, edge weight), tb[2e + 1] = (arena offset low 32 bits,
+// arena offset bits 32-47 | base code << 16 | preferred << 24, the row's
+// predecessor list start, its count). `preferred` is the reference's
+// preferred-match weight test of the entry's edge, weight >= (sum of the row's
+// incoming weights) / 10 (align.rs:1227-1228). An entry whose predecessor is
+// out of range or skipped has row -1.
+__device__ inline void fill_tb(Scratch &s, int n) {
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < n; i += 32) {
+    const int pb = s.pred_start[i], pc = s.pred_cnt[i];
+    const int64_t ws10 = s.wsum[i] / 10;
+    for (int t = 0; t < pc; ++t) {
+      const int2 pr = s.pred[pb + t];
+      int4 a = make_int4(-1, 0, 0, pr.y), b = make_int4(0, 0, 0, 0);
+      if (pr.x >= 0) {
+        const int p = pr.x;
+        const uint64_t off = uint64_t(s.row_off[p]);
+        a = make_int4(p, s.row_start[p], s.row_len[p], pr.y);
+        b = make_int4(int(off & 0xffffffffu),
+                      int(((off >> 32) & 0xffffu) | (uint32_t(s.row_base[p]) << 16) | (int64_t(pr.y) >= ws10 ? 1u << 24 : 0u)),
+                      s.pred_start[p], s.pred_cnt[p]);
+      }
+      s.tb[2 * (pb + t)] = a;
+      s.tb[2 * (pb + t) + 1] = b;
+    }
+  }
+  __syncwarp();
+}
+
 // Traceback of align.rs:1164-1347 by the whole warp, reading the stored DP
 // states. Each step is the reference's decision sequence (preferred match,
 // deletion open / extend, insertion open / extend, match); lane t examines
 // predecessor t of the current row in parallel, and the reference's choose()
 // -- the first predecessor of largest weight among those whose state explains
-// the cell -- becomes a ballot plus a max-reduction over the lanes. While the
-// predecessors' states are loaded, each lane also loads the row descriptor
-// its predecessor would need as the next row, so a step costs two dependent
-// memory round trips. Steps are recorded as (row, column, kind) and resolved
-// into AlignedBase items (push_diagonal, align.rs:1316-1347) by a parallel
-// pass at the end, which also reverses them and prepends the source.
+// the cell -- becomes a ballot plus a max-reduction over the lanes.
+//
+// A step costs one memory round trip: lane t holds predecessor t's
+// descriptor (fill_tb) in registers, so the states of the current cell and of
+// every predecessor cell are loaded at once, together with the descriptors of
+// the first two predecessors of each predecessor -- the next row's entries
+// whichever predecessor the step moves to; they reach their lanes by shuffle.
+// Steps are recorded as (row, column, kind) and resolved into AlignedBase
+// items (push_diagonal, align.rs:1316-1347) by a parallel pass at the end,
+// which also reverses them and prepends the source.
 template <typename S>
 __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A, int beg, int n, int64_t m,
-                             const int32_t *mat, int *n_out) {
+                             const int32_t *mat, const uint8_t *q8, int *n_out) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
   const int lane = threadIdx.x & 31;
   const int64_t neg_half = int64_t(NEGV) / 2;
   const int64_t O = P.gap_open, E = P.gap_ext;
   constexpr int KIND_INS = 0, KIND_DIAG = 1;
+  const int4 none = make_int4(-1, 0, 0, 0), zero = make_int4(0, 0, 0, 0);
+  fill_tb(s, n);
   int i = n - 1;
   int j = int(m - 1);
   int op = OP_ALL;
   int nres = 0;
   int64_t steps = 0;
   int4 *res = s.items;
-  // descriptor of the current row
+  // the current row and this lane's predecessor entry of it (lanes < pc)
   int rs = s.row_start[i], rl = s.row_len[i], pb = s.pred_start[i], pc = s.pred_cnt[i], rb = s.row_base[i];
-  int64_t ro = s.row_off[i], ws = s.wsum[i];
+  int64_t ro = s.row_off[i];
+  int4 ea = none, eb = zero;
+  if (lane < pc) {
+    ea = s.tb[2 * (pb + lane)];
+    eb = s.tb[2 * (pb + lane) + 1];
+  }
   auto at = [&](int64_t off, int start, int len, int plane, int c) -> int64_t {
     return (c >= start && c - start < len) ? int64_t(A[off + int64_t(plane) * len + (c - start)]) : int64_t(NEGV);
   };
+  auto eoff = [](const int4 &b) { return int64_t(uint64_t(uint32_t(b.x)) | (uint64_t(uint32_t(b.y) & 0xffffu) << 32)); };
   int32_t st = ST_OK;
   while (i > 0 || j > 0) {
     steps += 1;
@@ -870,93 +924,145 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
       st = ST_TB_NO_ADVANCE;
       break;
     }
-    const bool in_ij = j >= rs && j - rs < rl;
-    if (!in_ij) {
+    if (!(j >= rs && j - rs < rl)) {
       st = ST_TB_LEFT_BAND;
       break;
     }
+    // one round of loads: the current cell (and its left neighbour), every
+    // predecessor cell, and the predecessors' first two entries
     const int64_t Mij = at(ro, rs, rl, 0, j), Dij = at(ro, rs, rl, 1, j), Iij = at(ro, rs, rl, 2, j);
+    const int64_t Mim = at(ro, rs, rl, 0, j - 1), Iim = at(ro, rs, rl, 2, j - 1);
+    int64_t Mpm = NEGV, Mpj = NEGV, Dpj = NEGV;
+    int4 n0a = none, n0b = zero, n1a = none, n1b = zero;
+    const bool mine = lane < pc && ea.x >= 0;
+    if (mine) {
+      const int64_t po = eoff(eb);
+      Mpm = at(po, ea.y, ea.z, 0, j - 1);
+      Mpj = at(po, ea.y, ea.z, 0, j);
+      Dpj = at(po, ea.y, ea.z, 1, j);
+      if (eb.w > 0) {
+        n0a = s.tb[2 * eb.z];
+        n0b = s.tb[2 * eb.z + 1];
+      }
+      if (eb.w > 1) {
+        n1a = s.tb[2 * (eb.z + 1)];
+        n1b = s.tb[2 * (eb.z + 1) + 1];
+      }
+    }
     if (Mij <= neg_half) {
       st = ST_TB_LEFT_BAND;
       break;
     }
-    const int qb = s.seq[j];
+    const int qb = q8[j];
     const int64_t score = mat[rb * P.sigma + qb];
-    // per-predecessor flags, chunks of 32 predecessors (one in almost all rows)
-    int m_lane = -1, m_w = 0, o_lane = -1, o_w = 0, x_lane = -1, x_w = 0;  // best lane + weight per kind
+    // per-predecessor flags; best lane and weight per kind (chunk 0 from the
+    // registers, further chunks of 32 from memory)
+    int m_lane = -1, m_w = 0, o_lane = -1, o_w = 0, x_lane = -1, x_w = 0;
     int m_chunk = 0, o_chunk = 0, x_chunk = 0;
-    int4 pm = make_int4(-1, 0, 0, 0);
-    int64_t poff = 0;
-    int4 pnext = make_int4(0, 0, 0, 0);  // (pred_start, pred_cnt, row_base, -) of the lane's predecessor
-    int64_t pws = 0;
-    for (int t0 = 0; t0 < pc; t0 += 32) {
-      const int t = t0 + lane;
-      int4 q = make_int4(-1, 0, 0, 0);
-      int64_t qoff = 0;
-      if (t < pc) {
-        q = s.pmeta[pb + t];
-        qoff = s.pmeta_off[pb + t];
-      }
-      bool fm = false, fo = false, fx = false;
-      if (q.x >= 0 && t0 == 0) {
-        pnext = make_int4(s.pred_start[q.x], s.pred_cnt[q.x], s.row_base[q.x], 0);
-        pws = s.wsum[q.x];
-      }
-      if (q.x >= 0) {
-        const int64_t Mpm = at(qoff, q.y, q.z, 0, j - 1);
-        const int64_t Mpj = at(qoff, q.y, q.z, 0, j), Dpj = at(qoff, q.y, q.z, 1, j);
-        const bool c1 = j - 1 >= q.y && j - 1 - q.y < q.z, c0 = j >= q.y && j - q.y < q.z;
-        fm = j > 0 && c1 && Mij == Mpm + score;
-        fo = c0 && Dij == Mpj + O;
-        fx = c0 && Dij == Dpj + E;
-      }
-      auto best = [&](bool f, int &bl, int &bw, int &bc) {
-        const unsigned msk = __ballot_sync(FULL, f);
-        if (!msk) return;
-        const int mx = __reduce_max_sync(FULL, f ? unsigned(q.w) : 0u);
-        const int l = __ffs(__ballot_sync(FULL, f && q.w == mx)) - 1;
-        if (bl < 0 || mx > bw) {
-          bl = l;
-          bw = mx;
-          bc = t0;
-        }
-      };
-      best(fm, m_lane, m_w, m_chunk);
-      best(fo, o_lane, o_w, o_chunk);
-      best(fx, x_lane, x_w, x_chunk);
-      if (t0 == 0) {
-        pm = q;
-        poff = qoff;
-      }
-    }
-    // moves to predecessor (lane l of chunk c); the next row's descriptor
-    auto move_to = [&](int l, int c) {
-      int4 q = pm;
-      int64_t qoff = poff;
-      if (c != 0) {
-        const int t = c + lane;
-        if (t < pc) {
-          q = s.pmeta[pb + t];
-          qoff = s.pmeta_off[pb + t];
-        }
-      }
-      i = __shfl_sync(FULL, q.x, l);
-      rs = __shfl_sync(FULL, q.y, l);
-      rl = __shfl_sync(FULL, q.z, l);
-      ro = __shfl_sync(FULL, (long long)qoff, l);
-      if (c == 0) {
-        pb = __shfl_sync(FULL, pnext.x, l);
-        pc = __shfl_sync(FULL, pnext.y, l);
-        rb = __shfl_sync(FULL, pnext.z, l);
-        ws = __shfl_sync(FULL, (long long)pws, l);
-      } else {
-        pb = s.pred_start[i];
-        pc = s.pred_cnt[i];
-        rb = s.row_base[i];
-        ws = s.wsum[i];
+    auto best = [&](bool f, int w, int t0, int &bl, int &bw, int &bc) {
+      const unsigned msk = __ballot_sync(FULL, f);
+      if (!msk) return;
+      const int mx = __reduce_max_sync(FULL, f ? unsigned(w) : 0u);
+      const int l = __ffs(__ballot_sync(FULL, f && w == mx)) - 1;
+      if (bl < 0 || mx > bw) {
+        bl = l;
+        bw = mx;
+        bc = t0;
       }
     };
-    if ((op & OP_MATCH) && j > 0 && rb == qb && m_lane >= 0 && int64_t(m_w) >= ws / 10) {
+    auto flags = [&](const int4 &a, int64_t pm, int64_t pj, int64_t dj, bool &fm, bool &fo, bool &fx) {
+      const bool c1 = j - 1 >= a.y && j - 1 - a.y < a.z, c0 = j >= a.y && j - a.y < a.z;
+      fm = j > 0 && c1 && Mij == pm + score;
+      fo = c0 && Dij == pj + O;
+      fx = c0 && Dij == dj + E;
+    };
+    {
+      bool fm = false, fo = false, fx = false;
+      if (mine) flags(ea, Mpm, Mpj, Dpj, fm, fo, fx);
+      best(fm, ea.w, 0, m_lane, m_w, m_chunk);
+      best(fo, ea.w, 0, o_lane, o_w, o_chunk);
+      best(fx, ea.w, 0, x_lane, x_w, x_chunk);
+    }
+    for (int t0 = 32; t0 < pc; t0 += 32) {  // rows with more than 32 predecessors
+      const int t = t0 + lane;
+      int4 qa = none, qbd = zero;
+      if (t < pc) {
+        qa = s.tb[2 * (pb + t)];
+        qbd = s.tb[2 * (pb + t) + 1];
+      }
+      bool fm = false, fo = false, fx = false;
+      if (qa.x >= 0) {
+        const int64_t po = eoff(qbd);
+        flags(qa, at(po, qa.y, qa.z, 0, j - 1), at(po, qa.y, qa.z, 0, j), at(po, qa.y, qa.z, 1, j), fm, fo, fx);
+      }
+      best(fm, qa.w, t0, m_lane, m_w, m_chunk);
+      best(fo, qa.w, t0, o_lane, o_w, o_chunk);
+      best(fx, qa.w, t0, x_lane, x_w, x_chunk);
+    }
+    // moves to predecessor (lane l of chunk c): its descriptor becomes the
+    // current row, its first two entries come from lane l's prefetch
+    auto move_to = [&](int l, int c) {
+      int4 qa = ea, qbd = eb;
+      if (c != 0) {
+        const int t = c + lane;
+        qa = none;
+        qbd = zero;
+        if (t < pc) {
+          qa = s.tb[2 * (pb + t)];
+          qbd = s.tb[2 * (pb + t) + 1];
+        }
+      }
+      i = __shfl_sync(FULL, qa.x, l);
+      rs = __shfl_sync(FULL, qa.y, l);
+      rl = __shfl_sync(FULL, qa.z, l);
+      const int bx = __shfl_sync(FULL, qbd.x, l), by = __shfl_sync(FULL, qbd.y, l);
+      pb = __shfl_sync(FULL, qbd.z, l);
+      pc = __shfl_sync(FULL, qbd.w, l);
+      ro = int64_t(uint64_t(uint32_t(bx)) | (uint64_t(uint32_t(by) & 0xffffu) << 32));
+      rb = int((uint32_t(by) >> 16) & 0xffu);
+      int4 na = none, nb = zero;
+      if (c == 0) {
+        const int4 a0 = make_int4(__shfl_sync(FULL, n0a.x, l), __shfl_sync(FULL, n0a.y, l),
+                                  __shfl_sync(FULL, n0a.z, l), __shfl_sync(FULL, n0a.w, l));
+        const int4 b0 = make_int4(__shfl_sync(FULL, n0b.x, l), __shfl_sync(FULL, n0b.y, l),
+                                  __shfl_sync(FULL, n0b.z, l), __shfl_sync(FULL, n0b.w, l));
+        if (lane == 0) {
+          na = a0;
+          nb = b0;
+        }
+        if (pc > 1) {
+          const int4 a1 = make_int4(__shfl_sync(FULL, n1a.x, l), __shfl_sync(FULL, n1a.y, l),
+                                    __shfl_sync(FULL, n1a.z, l), __shfl_sync(FULL, n1a.w, l));
+          const int4 b1 = make_int4(__shfl_sync(FULL, n1b.x, l), __shfl_sync(FULL, n1b.y, l),
+                                    __shfl_sync(FULL, n1b.z, l), __shfl_sync(FULL, n1b.w, l));
+          if (lane == 1) {
+            na = a1;
+            nb = b1;
+          }
+        }
+        if (lane >= 2 && lane < pc) {
+          na = s.tb[2 * (pb + lane)];
+          nb = s.tb[2 * (pb + lane) + 1];
+        }
+      } else if (lane < pc) {
+        na = s.tb[2 * (pb + lane)];
+        nb = s.tb[2 * (pb + lane) + 1];
+      }
+      ea = na;
+      eb = nb;
+    };
+    const bool pref_ok = m_lane >= 0 &&
+                         ((uint32_t(__shfl_sync(FULL, m_chunk == 0 ? eb.y : 0, m_lane)) >> 24) & 1u) != 0;
+    bool pref = false;
+    if ((op & OP_MATCH) && j > 0 && rb == qb && m_lane >= 0) {
+      if (m_chunk == 0) {
+        pref = pref_ok;
+      } else {
+        const int t = m_chunk + m_lane;
+        pref = ((uint32_t(s.tb[2 * (pb + t) + 1].y) >> 24) & 1u) != 0;
+      }
+    }
+    if (pref) {
       if (lane == 0) res[nres] = make_int4(i, j, KIND_DIAG, 0);
       ++nres;
       move_to(m_lane, m_chunk);
@@ -977,7 +1083,6 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
       }
     }
     if ((op & OP_INSERT) && j > 0 && j - 1 >= rs && (op == OP_INSERT || Mij == Iij)) {
-      const int64_t Mim = at(ro, rs, rl, 0, j - 1), Iim = at(ro, rs, rl, 2, j - 1);
       if (Iij == Mim + O) {
         if (lane == 0) res[nres] = make_int4(i, j, KIND_INS, 0);
         ++nres;
@@ -1013,7 +1118,7 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
   // resolve, reverse, drop the sink entry (pushed first) and prepend the
   // source: final[k] = resolve(pushed[nres - k]) for k = 1..nres-1
   auto resolve = [&](int4 r) -> int4 {
-    const int qb = s.seq[r.y];
+    const int qb = q8[r.y];
     if (r.z == KIND_INS || (r.x == n - 1 && r.y != m - 1)) return make_int4(-1, qb, -1, 0);
     const int node = J->rank_to_node[beg + r.x];
     const int nb = J->base[node];
@@ -1500,14 +1605,18 @@ __device__ __forceinline__ int4 ld_early(const int4 *p) {
   return v;
 }
 
-// Static-band row plan (warp-wide), after fill_pmeta: per row its band,
-// predecessor list, arena offset, base code and ring entry, and per
-// predecessor entry where its states are: the ring entry of the
-// predecessor's first column when its states are still in the ring (the
-// predecessor and every row after it went through the ring, and at most
-// RING_CAP entries were written since), else -1, plus its arena offset. A row
-// goes through the ring when `ring` is set, its band is at most RING_MAX_LEN
-// and it has at most 32 predecessors (row 0: when its band fits).
+// Static-band row plan (warp-wide), after fill_pmeta. Per row (planc):
+// band start and length, predecessor list start and count, and the base
+// code it scores with. Per predecessor entry (pent), where the predecessor's
+// M and D states are: still in the ring (the predecessor and every row after
+// it went through the ring, and at most RING_CAP entries were written since)
+// as (ring entry of its first column, band start, band length, row), or in
+// the arena as (-1 - cum_hi, band start, band length, cum_lo) with cum the
+// predecessor's cumulative band length (its arena offset is 3 x cum); an
+// entry whose predecessor is skipped has band length 0. A row goes through
+// the ring when `ring` is set, its band is at most RING_MAX_LEN and it has at
+// most 32 predecessors (row 0: when its band fits). Counts the row kinds and
+// the predecessors read from the arena into `w`.
 __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w) {
   const int lane = threadIdx.x & 31;
   int carry = 0;  // rows before this block that did not go through the ring
@@ -1522,10 +1631,7 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w)
         g4 += fast && len > 384 ? 1 : 0;
         gen += fast ? 0 : 1;
       }
-      const int64_t off = s.row_off[i];
-      s.plan[i] = make_int4(s.row_start[i], len, s.pred_start[i], pc);
-      s.plan2[i] = make_int4(int(uint64_t(off) & 0xffffffffu), int(uint64_t(off) >> 32), s.row_base[i],
-                             int((off / 3) % cap));
+      s.planc[i] = make_int4(s.row_start[i], len, s.pred_start[i], int(uint32_t(pc) | (uint32_t(s.row_base[i]) << 24)));
     }
     const unsigned slow = __ballot_sync(FULL, i < n && !fast);
     if (i < n) s.nf[i] = carry + __popc(slow & ((1u << lane) - 1u));  // non-ring rows among 0..i-1
@@ -1538,10 +1644,17 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w)
     for (int t = 0; t < pc; ++t) {
       const int4 m = s.pmeta[pb + t];
       const int64_t po = s.pmeta_off[pb + t];
-      int pos = -1;
-      if (m.x >= 0 && m.z > 0 && s.nf[m.x] == nfi && off - po <= 3 * int64_t(cap)) pos = int((po / 3) % cap);
-      if (m.x >= 0 && m.z > 0 && pos < 0 && s.row_len[i] > 0 && s.row_len[i] <= RING_MAX_LEN) ++far;
-      s.pmeta2[pb + t] = make_int4(pos, int(uint64_t(po) & 0xffffffffu), int(uint64_t(po) >> 32), 0);
+      int4 e = make_int4(-1, 0, 0, 0);
+      if (m.x >= 0 && m.z > 0) {
+        if (s.nf[m.x] == nfi && off - po <= 3 * int64_t(cap)) {
+          e = make_int4(int((po / 3) % cap), m.y, m.z, m.x);
+        } else {
+          const uint64_t cum = uint64_t(po / 3);
+          e = make_int4(-1 - int(cum >> 31), m.y, m.z, int(cum & 0x7fffffffu));
+          if (s.row_len[i] > 0 && s.row_len[i] <= RING_MAX_LEN) ++far;
+        }
+      }
+      s.pent[pb + t] = e;
     }
   }
   __syncwarp();
@@ -1624,7 +1737,10 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   const S E = S(P.gap_ext), O = S(P.gap_open);
   const S s00 = S(P.matrix[P.unknown * P.sigma + P.unknown]);
   __syncwarp();
+  const uint64_t t_g0 = phase_clock();
   int32_t st = guides(J, s, beg, end, n, sm ? sm->gring_v : nullptr, sm ? sm->gring_s : nullptr);
+  const uint64_t t_g1 = phase_clock();
+  cells->phase[0] += t_g1 - t_g0;
   if (st != ST_OK) return st;
   const bool do_adapt = f != 0 && adaptive;
   if (do_adapt) {
@@ -1741,39 +1857,58 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
       }
       coop_bar(2);
     }
-    // rows 1..n-1, software-pipelined: row i+2's plan and row i+1's
-    // predecessor entries are loaded while row i computes
+    // rows 1..n-1. The plans of a 64-row window sit in the lanes (rows
+    // w0 + lane and w0 + 32 + lane), loaded 32 rows before they are needed;
+    // each row's predecessor entries are loaded three rows ahead. A row's
+    // arena offset and ring entry follow from the cumulative band length, so
+    // no global load stands between one row and the next.
     const int4 zero = make_int4(0, 0, 0, 0), none = make_int4(-1, 0, 0, 0);
-    int4 pa1 = n > 1 ? ld_early(s.plan + 1) : zero, pb1 = n > 1 ? ld_early(s.plan2 + 1) : zero;
-    int4 pa2 = n > 2 ? ld_early(s.plan + 2) : zero, pb2 = n > 2 ? ld_early(s.plan2 + 2) : zero;
-    int4 q1 = none, r1 = zero;
-    if (n > 1 && lane < pa1.w) {
-      q1 = ld_early(s.pmeta + pa1.z + lane);
-      r1 = ld_early(s.pmeta2 + pa1.z + lane);
-    }
+    int w0 = 0;
+    int4 wc = lane < n ? ld_early(s.planc + lane) : zero;
+    int4 wn = 32 + lane < n ? ld_early(s.planc + 32 + lane) : zero;
+    auto pent_of = [&](int r) {  // r - w0 < 64
+      if (r >= n) return none;
+      const int d = r - w0;
+      const int4 v = d < 32 ? wc : wn;
+      const int pb = __shfl_sync(FULL, v.z, d & 31);
+      const int pc = __shfl_sync(FULL, v.w, d & 31) & 0xffffff;
+      return lane < pc ? ld_early(s.pent + pb + lane) : none;
+    };
+    int4 e1 = pent_of(1), e2 = pent_of(2), e3 = pent_of(3);
+    int64_t cum = s.row_len[0];  // cumulative band length of the rows before row i
+    int rpos = rcap > 0 ? int(cum % rcap) : 0;
     for (int i = 1; i < n; ++i) {
-      const int4 a = pa1, b = pb1, mt = q1, mr = r1;
-      pa1 = pa2;
-      pb1 = pb2;
-      q1 = none;
-      r1 = zero;
-      if (i + 1 < n && lane < pa1.w) {
-        q1 = ld_early(s.pmeta + pa1.z + lane);
-        r1 = ld_early(s.pmeta2 + pa1.z + lane);
+      if (i - w0 >= 32) {
+        w0 += 32;
+        wc = wn;
+        wn = w0 + 32 + lane < n ? ld_early(s.planc + w0 + 32 + lane) : zero;
       }
-      if (i + 2 < n) {
-        pa2 = ld_early(s.plan + i + 2);
-        pb2 = ld_early(s.plan2 + i + 2);
-      }
-      const int start = a.x, len = a.y, pb = a.z, pc = a.w;
+      const int src = (i - w0) & 31;
+      const int start = __shfl_sync(FULL, wc.x, src), len = __shfl_sync(FULL, wc.y, src);
+      const int pb = __shfl_sync(FULL, wc.z, src);
+      const uint32_t pcw = uint32_t(__shfl_sync(FULL, wc.w, src));
+      const int pc = int(pcw & 0xffffffu), base = int(pcw >> 24);
+      const int4 mt = e1;
+      e1 = e2;
+      e2 = e3;
+      e3 = pent_of(i + 3);
       if (len == 0) continue;
-      const int64_t off = int64_t((uint64_t(uint32_t(b.y)) << 32) | uint32_t(b.x));
-      const int base = b.z;
+      const int64_t off = 3 * cum;
+      const int pos_i = rpos;
+      cum += len;
+      if (rcap > 0) {
+        if (len < rcap) {
+          rpos += len;
+          if (rpos >= rcap) rpos -= rcap;
+        } else {
+          rpos = int(cum % rcap);
+        }
+      }
       S *R = A + off;
       if (ring && len <= RING_MAX_LEN && pc <= 32) {
-        const bool ok = mt.x >= 0 && mt.z > 0;
-        const int64_t mo = int64_t((uint64_t(uint32_t(mr.z)) << 32) | uint32_t(mr.y));
-        const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + mo;
+        const bool ok = mt.z > 0;
+        const int64_t mcum = mt.x < 0 ? ((int64_t(-1 - mt.x) << 31) | int64_t(uint32_t(mt.w))) : 0;
+        const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + 3 * mcum;
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         if (coop) {
@@ -1781,14 +1916,14 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
           if (ok) {
             cd->ps[slot] = mt.y;
             cd->pl[slot] = mt.z;
-            cd->pos[slot] = mr.x;
+            cd->pos[slot] = mt.x < 0 ? -1 : mt.x;
             cd->g[slot] = my_g;
           }
           if (lane == 0) {
             cd->op = COOP_ROW;
             cd->start = start;
             cd->len = len;
-            cd->pos_i = b.w;
+            cd->pos_i = pos_i;
             cd->n_pred = __popc(vmask);
             cd->R = reinterpret_cast<int32_t *>(R);
             cd->mrow = mrow;
@@ -1800,7 +1935,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
         dp_row_fast<false>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
-                           mt.y, mt.z, ok ? mr.x : -1, my_g, rm, rd, rcap, b.w, bv, bj);
+                           mt.y, mt.z, (ok && mt.x >= 0) ? mt.x : -1, my_g, rm, rd, rcap, pos_i, bv, bj);
         __syncwarp();
         continue;
       }
@@ -1920,7 +2055,10 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     fill_pmeta(s, n);
     cells->pred_cells += pred_overlap_cells(s, n);
   }
-  st = traceback<S>(J, P, s, A, beg, n, m, (sm && smem_matrix) ? sm->matrix : P.matrix, n_items);
+  const uint64_t t_d1 = phase_clock();
+  cells->phase[1] += t_d1 - t_g1;
+  st = traceback<S>(J, P, s, A, beg, n, m, (sm && smem_matrix) ? sm->matrix : P.matrix, q8, n_items);
+  cells->phase[2] += phase_clock() - t_d1;
   return st;
 }
 
@@ -2203,6 +2341,7 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   Work cells{};
   int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, sm);
   if (st != ST_OK) return st;
+  const uint64_t t_u0 = phase_clock();
   const int n_old = J->n_nodes;
   int32_t *mark = s.dp_bytes >= int64_t(n_old) * 4 ? reinterpret_cast<int32_t *>(s.dp) : nullptr;
   if (!add_path_warp(J, P, r, s.items, n_items, &st, mark)) {
@@ -2235,6 +2374,8 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
       J->rows_g4 += cells.rows_g4;
       J->rows_generic += cells.rows_generic;
       J->coop |= cells.coop;
+      cells.phase[3] += phase_clock() - t_u0;
+      for (int k = 0; k < 4; ++k) J->phase[k] += cells.phase[k];
       J->next_read = r + 1;
     }
   }

@@ -20,6 +20,7 @@
 #include "../../include/minipoa_b200.h"
 #include "host_graph.h"
 #include "poa_internal.h"
+#include "poa_consensus.h"
 #include "poa_pack.h"
 #include "seed.h"
 
@@ -756,6 +757,67 @@ struct poa_batch {
     CK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, ctx->stream));
   }
 
+  // Consensus FASTA of every set, computed on the device (poa_consensus.cu):
+  // only the consensus bases leave the GPU. A failed set gets its error line.
+  std::vector<std::string> device_consensus() {
+    download_jobs();
+    const size_t nj = jobs.size();
+    std::vector<int64_t> scr(nj + 1, 0), oo(nj + 1, 0);
+    for (size_t s = 0; s < nj; ++s) {
+      scr[s + 1] = scr[s] + consensus_scratch_bytes(jobs[s].n_nodes, jobs[s].n_edges);
+      oo[s + 1] = oo[s] + (int64_t(jobs[s].n_nodes) + 15) / 16 * 16;
+    }
+    const size_t scr_bytes = size_t(scr.back()), out_bytes = size_t(oo.back());
+    std::vector<uint8_t> dec(256, 'N');
+    for (int c = 0; c < sigma; ++c) dec[size_t(c)] = hp.decode(c);
+    // scratch: the DP arena pool when it holds it, else its own allocation
+    const bool own = !(arenas && arena_pool >= int64_t(scr_bytes));
+    char *d_scr = own ? (char *)ctx->dalloc(scr_bytes + 16) : arenas;
+    uint8_t *d_out = nullptr, *d_dec = nullptr;
+    int64_t *d_so = nullptr, *d_oo = nullptr;
+    int32_t *d_len = nullptr;
+    std::vector<int32_t> len(nj);
+    std::vector<uint8_t> bytes(out_bytes + 1);
+    auto release = [&] {
+      if (own) ctx->dfree(d_scr, scr_bytes + 16);
+      ctx->dfree(d_out, out_bytes + 16);
+      ctx->dfree(d_dec, 256);
+      ctx->dfree(d_so, (nj + 1) * 8);
+      ctx->dfree(d_oo, (nj + 1) * 8);
+      ctx->dfree(d_len, nj * 4 + 4);
+    };
+    try {
+      d_out = (uint8_t *)ctx->dalloc(out_bytes + 16);
+      d_dec = (uint8_t *)ctx->dalloc(256);
+      d_so = (int64_t *)ctx->dalloc((nj + 1) * 8);
+      d_oo = (int64_t *)ctx->dalloc((nj + 1) * 8);
+      d_len = (int32_t *)ctx->dalloc(nj * 4 + 4);
+      CK(cudaMemcpyAsync(d_dec, dec.data(), 256, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(d_so, scr.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(d_oo, oo.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+      CK(launch_consensus(d_jobs, int(nj), d_dec, d_scr, d_so, d_out, d_oo, d_len, ctx->stream));
+      CK(cudaMemcpyAsync(len.data(), d_len, nj * 4, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaMemcpyAsync(bytes.data(), d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      d2h_bytes = out_bytes + nj * 4 + jobs.size() * sizeof(Job);
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+    std::vector<std::string> parts(nj);
+    for (size_t s = 0; s < nj; ++s) {
+      const Job &J = jobs[s];
+      if (J.status != ST_OK || len[s] < 0) {
+        parts[s] = "!error " + status_message(J.status, J.err_i, J.err_j) + "\n";
+        continue;
+      }
+      const char *b0 = reinterpret_cast<const char *>(bytes.data() + oo[s]);
+      parts[s] = ">consensus sequence\n" + std::string(b0, b0 + len[s]) + "\n";
+    }
+    return parts;
+  }
+
   // Packs the graphs of `ids` and parses them on the host.
   std::vector<HostGraph> graphs(const std::vector<int32_t> &ids) {
     download_jobs();
@@ -1320,6 +1382,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
     b->download_jobs();
     b->ran = true;
     if (stats) {
+      for (int k = 0; k < 4; ++k) stats->phase_cycles[k] = 0;
       uint64_t cells = 0, reads = 0, dpb = 0, pc = 0, far = 0, g4 = 0, gen = 0;
       int32_t coop = 0;
       for (auto &J : b->jobs) {
@@ -1331,6 +1394,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
         g4 += J.rows_g4;
         gen += J.rows_generic;
         coop += J.coop;
+        for (int k = 0; k < 4; ++k) stats->phase_cycles[k] += J.phase[k];
       }
       stats->cells = cells;
       stats->dp_bytes = dpb;
@@ -1400,6 +1464,17 @@ int poa_batch_output_all(poa_ctx *ctx, poa_batch *b, int32_t result, char **out,
   *out_len = 0;
   return api(ctx, [&] {
     if (result != 0 && result != 2) throw AlignError{POA_ERR_INVALID, "batch output supports results 0 and 2"};
+    if (result == 0) {  // consensus on the device: only the sequences come back
+      auto parts = b->device_consensus();
+      size_t total = 0;
+      for (auto &p : parts) total += p.size();
+      std::string all;
+      all.reserve(total);
+      for (auto &p : parts) all += p;
+      *out = dup_string(all);
+      *out_len = int64_t(all.size());
+      return;
+    }
     std::vector<int32_t> ids(static_cast<size_t>(b->n_sets));
     std::iota(ids.begin(), ids.end(), 0);
     auto gs = b->graphs(ids);

@@ -330,6 +330,7 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   J->rows_g4 = 0;
   J->rows_generic = 0;
   J->coop = 0;
+  for (int k = 0; k < 4; ++k) J->phase[k] = 0;
   J->order_exact = 1;
 }
 

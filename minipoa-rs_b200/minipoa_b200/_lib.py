@@ -54,7 +54,8 @@ class BatchStats(ctypes.Structure):
                 ("launches", ctypes.c_int32), ("relaunches", ctypes.c_int32), ("slots", ctypes.c_int32),
                 ("reserved", ctypes.c_int32), ("kernel_ms", ctypes.c_double), ("dp_bytes", ctypes.c_uint64),
                 ("pred_cells", ctypes.c_uint64), ("far_preds", ctypes.c_uint64), ("rows_g4", ctypes.c_uint64),
-                ("rows_generic", ctypes.c_uint64), ("coop_jobs", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
+                ("rows_generic", ctypes.c_uint64), ("coop_jobs", ctypes.c_int32), ("reserved2", ctypes.c_int32),
+                ("phase_cycles", ctypes.c_uint64 * 4)]
 
 
 # name -> (restype, argtypes); every function declared in include/minipoa_b200.h
