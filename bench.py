@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--mem-budget-gb", type=float, default=0.0,
                     help="device memory budget of the context (0: 90%% of free memory)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (small profiling runs)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the single-set and protein configurations")
+    ap.add_argument("--split", action="store_true",
+                    help="N>1: split one list of --sets sets over the ranks (strong scaling) instead of "
+                         "--sets sets per rank (weak scaling)")
     ap.add_argument("--serve-jobs", type=int, default=1024, help="jobs of the serving loop's saturation run (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="length of the serving run at 80%% load")
     ap.add_argument("--seeded-reads", type=int, default=20,
@@ -335,6 +339,68 @@ def seeded_bench(mp, ctx, n_reads: int, seed: int = 1002):
     return out
 
 
+def c1_bench(mp, ctx, params, reps: int = 5):
+    """One 1,000 bp x 20-read set (seed 1001; 1% sub, 0.5% ins, 0.5% del),
+    consensus output, through the single-graph API (align_sequences: every
+    read of the set in one launch, graph resident on the device), against the
+    oracle's AVX2 kernel on one thread (the reference's unseeded runs are
+    single-threaded whatever -t is). Latency per set and GCUPS; consensus
+    bytes compared."""
+    import oracle
+    from minipoa_b200 import workloads
+
+    reads = workloads.unseeded_consensus_set(1001)
+    mp.align_sequences(params, reads, ctx).consensus(params)  # warm-up
+    ts, cons = [], None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        g = mp.align_sequences(params, reads, ctx)
+        cons = g.consensus(params)[0]
+        ts.append(time.perf_counter() - t0)
+    oracle.reset_cells()
+    t0 = time.perf_counter()
+    o = oracle.align_sequences(params, reads, kernel=oracle.AUTO_AVX2)
+    tc = time.perf_counter() - t0
+    cells = oracle.cells()
+    t = statistics.median(ts)
+    return {"workload": "1,000 bp ancestor x 20 reads (seed 1001), -r0, default Params",
+            "cells": cells, "gpu_ms_per_set": t * 1e3, "gpu_gcups": cells / t / 1e9,
+            "timing": f"host wall clock through the C ABI (upload, all reads, download, consensus), median of {reps}",
+            "cpu_1thread_ms": tc * 1e3, "cpu_1thread_gcups": cells / tc / 1e9,
+            "consensus_identical": cons == o.consensus(params)[0]}
+
+
+def c4a_bench(mp, ctx, n_fam: int = 1000, threads: int = 0):
+    """Protein families (-f0 full DP, 20-letter alphabet, symmetric integer
+    matrix): 1,000 families x 30 members of 300-800 residues at 20%
+    divergence, in one batched launch; the oracle's AVX2 kernel on all host
+    threads over a stratified sample of the families; consensus bytes of the
+    sample compared."""
+    import oracle
+    from minipoa_b200 import workloads
+    from minipoa_b200.params import Params
+
+    threads = threads or os.cpu_count() or 1
+    fams = workloads.protein_families(n_fam)
+    params = Params(alphabet=workloads.PROTEIN_ALPHABET, matrix=workloads.protein_matrix(), f=0)
+    b = mp.Batch(params, fams, ctx)
+    b.run(0)
+    st = b.run(0)
+    out = b.output_all(0)
+    sample = list(range(0, n_fam, max(1, n_fam // (4 * threads))))
+    t0 = time.perf_counter()
+    cells, hashes = oracle.batch_run(params, [fams[s] for s in sample], kernel=oracle.AUTO_AVX2, threads=threads,
+                                     out_format=0)
+    tc = time.perf_counter() - t0
+    par = consensus_parity(out, dict(zip(sample, hashes)))
+    del b
+    return {"workload": f"{n_fam} protein families x 30 (300-800 aa, 15% sub + 5% indels), -f0, 20x20 matrix",
+            "cells": st.cells, "gpu_ms": st.device_ms, "gpu_gcups": st.cells / st.device_ms / 1e6,
+            "rows_generic": st.rows_generic,
+            "cpu": {"gcups": cells / tc / 1e9, "cores": threads, "sample": f"{len(sample)} families"},
+            "parity": par}
+
+
 def load_traffic():
     """DRAM bytes per launch of the batched kernel from the committed ncu
     summary, scaled to this run's cells (null when absent)."""
@@ -353,7 +419,17 @@ def main():
     from minipoa_b200.params import Params
 
     params = Params()
-    sets = workloads.batched_sets(args.sets, seed=args.seed + rank, lmax=args.lmax, dmax=args.dmax)
+    if args.split and world > 1:
+        # strong scaling: one list of sets split over the ranks by estimated
+        # work (minipoa_b200.shard), the same split computed on every rank
+        from minipoa_b200 import shard
+
+        every = workloads.batched_sets(args.sets, seed=args.seed, lmax=args.lmax, dmax=args.dmax)
+        share = shard.partition([shard.set_work(x) for x in every], world)[rank]
+        sets = [every[s] for s in share]
+        del every
+    else:
+        sets = workloads.batched_sets(args.sets, seed=args.seed + rank, lmax=args.lmax, dmax=args.dmax)
 
     if args.impl == "reference":
         if rank != 0:
@@ -459,6 +535,17 @@ def main():
         except Exception as e:  # the throughput line above stands on its own
             serving = {"error": str(e)}
 
+    c1 = c4a = None
+    if rank == 0 and not args.no_extra:
+        try:
+            c1 = c1_bench(mp, ctx, params)
+        except Exception as e:
+            c1 = {"error": str(e)}
+        try:
+            c4a = c4a_bench(mp, ctx)
+        except Exception as e:
+            c4a = {"error": str(e)}
+
     seeded = None
     if rank == 0 and args.seeded_reads > 0:
         try:
@@ -498,7 +585,8 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "scaling": "strong" if (args.split and world > 1) else "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD.replace("200-5000", f"200-{args.lmax}").replace("10-60", f"10-{args.dmax}"),
                        "sets": args.sets, "seed": args.seed, "reads_per_step": reads // args.steps,
                        "cells_per_step": cells // args.steps, "l2": "inputs larger than L2 (no flush needed)",
@@ -517,6 +605,8 @@ def main():
             "plain_vs_batched": plain,
             "serving": serving,
             "seeded": seeded,
+            "c1_single_set": c1,
+            "c4a_protein": c4a,
         }
         print(json.dumps(line))
     if pg is not None:

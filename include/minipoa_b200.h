@@ -277,6 +277,18 @@ void poa_batch_free(poa_batch *batch);
  * over every SM. Allocates a small device buffer; about 0.1 s. */
 int poa_probe_int_peak(int32_t device, double *out_ops_per_s);
 
+/* io::read_gfa (called at src/lib.rs:214-218; its source file is absent from
+ * the reference tree, so the behaviour follows tests/io_cli.rs:374-431,
+ * 563-610): GFA text -> a device graph ranked by the LIFO toposort, and its
+ * path records as library-owned "name\tsequence\n" lines (one per P line,
+ * in file order). Segments become chains of single-base nodes; only forward
+ * links with a 0M overlap are accepted; duplicate segments, unknown
+ * references, reverse orientations, self links, cycles and paths revisiting
+ * a node ("revisits") are POA_ERR_ALIGN with the reason. Extending the graph
+ * with new reads is poa_extend_graph with existing = the record count. */
+int poa_graph_read_gfa(poa_ctx *ctx, const poa_params *params, const char *text, int64_t len, poa_graph **out,
+                       char **records, int64_t *records_len);
+
 /* Tuning: concurrent warp slots per SM for the batched kernel (0 = auto) and
  * the DP arena bytes per slot (0 = auto from the budget). */
 int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot);
@@ -325,6 +337,13 @@ int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_byte
 /* Queues one job (its reads in order); returns at once with its id. */
 int poa_server_submit(poa_ctx *ctx, poa_server *server, int64_t n_seqs, const uint8_t *const *seqs,
                       const int64_t *lens, int64_t *job_id);
+/* Queues one job that extends an initial graph given as GFA text (the
+ * reference's -i workflow, src/lib.rs:214-231, with progressive ordering
+ * off): the GFA is parsed and ranked at once (errors as poa_graph_read_gfa),
+ * copied into device memory when the job is admitted, and the reads are
+ * aligned into it; their sequence ids follow the GFA's path records. */
+int poa_server_submit_gfa(poa_ctx *ctx, poa_server *server, const char *gfa, int64_t gfa_len, int64_t n_seqs,
+                          const uint8_t *const *seqs, const int64_t *lens, int64_t *job_id);
 /* Waits for a job to finish (timeout_ms < 0: no limit; POA_ERR_TIMEOUT when
  * it runs out). */
 int poa_server_wait(poa_ctx *ctx, poa_server *server, int64_t job, double timeout_ms, int32_t *state);

@@ -37,7 +37,6 @@ __global__ void k_consensus(const Job *jobs, int n_jobs, const uint8_t *decode, 
     return;
   }
   const int n = J.n_nodes;
-  const int64_t e = J.n_edges;
   auto up = [](int64_t x) { return (x + 15) / 16 * 16; };
   char *base = scratch + scr_off[w];
   uint64_t *score = reinterpret_cast<uint64_t *>(base);

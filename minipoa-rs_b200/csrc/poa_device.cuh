@@ -48,6 +48,7 @@ enum Status : int32_t {
   ST_ARENA_FULL = 100,
   ST_GRAPH_FULL = 101,
   ST_SEEDING_UNSUPPORTED = 102,
+  ST_OUT_TOO_SMALL = 103,  // a caller's output buffer holds fewer items than the path
 };
 
 __host__ __device__ inline bool is_alignment_error(int32_t s) { return s > 0 && s < 100; }
@@ -95,6 +96,7 @@ struct Job {
   const int64_t *read_off;
   const int32_t *read_len;
   int32_t n_reads, next_read;
+  int32_t seq_base;  // sequence id of read 0 (reads extending an imported graph follow its records)
   // outcome
   int32_t status, err_i, err_j, n_items;
   int32_t order_exact;  // 1 when rank is the reference's LIFO toposort order
@@ -729,6 +731,10 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
     const int count = n - 1;  // rows 1..n-1 forward, n-2..0 backward
     auto row_of = [&](int q) { return first + step * q; };
     Lists nxt = load(st, ct, ent, row_of(lane), lane < count);
+    // the row computed last (row 0 forward, row n-1 backward, to begin
+    // with): most rows' best candidate is that row, read from registers
+    int last = forward ? 0 : n - 1;
+    int64_t last_v = rv[last & (GRING - 1)], last_s = rsu[last & (GRING - 1)];
     for (int q0 = 0; q0 < count; q0 += 32) {
       const Lists cur = nxt;
       nxt = load(st, ct, ent, row_of(q0 + 32 + lane), q0 + 32 + lane < count);
@@ -746,6 +752,11 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
         f0 = make_int2(__shfl_sync(FULL, cur.e0.x, kn), __shfl_sync(FULL, cur.e0.y, kn));
         f1 = make_int2(__shfl_sync(FULL, cur.e1.x, kn), __shfl_sync(FULL, cur.e1.y, kn));
         auto get = [&](int x, int64_t &v, int64_t &sp) {
+          if (x == last) {
+            v = last_v;
+            sp = last_s;
+            return;
+          }
           const bool near = (forward ? i - x : x - i) < GRING;
           v = near ? rv[x & (GRING - 1)] : val[x];
           sp = near ? rsu[x & (GRING - 1)] : s.support[x];
@@ -787,6 +798,9 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
         }
         rv[i & (GRING - 1)] = vi;
         rsu[i & (GRING - 1)] = si;
+        last = i;
+        last_v = vi;
+        last_s = si;
       }
     }
   };
@@ -2344,8 +2358,8 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   const uint64_t t_u0 = phase_clock();
   const int n_old = J->n_nodes;
   int32_t *mark = s.dp_bytes >= int64_t(n_old) * 4 ? reinterpret_cast<int32_t *>(s.dp) : nullptr;
-  if (!add_path_warp(J, P, r, s.items, n_items, &st, mark)) {
-    if (lane == 0) st = add_path(J, P, r, s.items, n_items);
+  if (!add_path_warp(J, P, J->seq_base + r, s.items, n_items, &st, mark)) {
+    if (lane == 0) st = add_path(J, P, J->seq_base + r, s.items, n_items);
     st = __shfl_sync(FULL, st, 0);
   }
   __syncwarp();

@@ -11,6 +11,7 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <stdexcept>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -20,6 +21,7 @@
 #include "../../include/minipoa_b200.h"
 #include "host_graph.h"
 #include "poa_internal.h"
+#include "gfa.h"
 #include "poa_consensus.h"
 #include "poa_pack.h"
 #include "seed.h"
@@ -63,6 +65,7 @@ std::string status_message(int32_t st, int err_i, int err_j) {
     case ST_COLUMN_DEPS: return "invalid graph column dependencies";
     case ST_ARENA_FULL: return "DP arena exhausted";
     case ST_GRAPH_FULL: return "graph capacity exhausted";
+    case ST_OUT_TOO_SMALL: return "output buffer holds fewer items than the alignment path";
     case ST_SEEDING_UNSUPPORTED: return "seeded windows (-S) are not available in this build";
     default: return "unknown device status " + std::to_string(st);
   }
@@ -71,6 +74,7 @@ std::string status_message(int32_t st, int err_i, int err_j) {
 int status_code(int32_t st) {
   if (is_alignment_error(st)) return POA_ERR_ALIGN;
   if (st == ST_SEEDING_UNSUPPORTED) return POA_ERR_UNSUPPORTED;
+  if (st == ST_OUT_TOO_SMALL) return POA_ERR_INVALID;
   return POA_ERR_ALLOC;
 }
 
@@ -392,6 +396,138 @@ poa_graph *new_graph(poa_ctx *ctx, const HostParams &hp, Caps caps) {
   g->upload();
   CK(launch_reset(g->d_job, 1, g->sigma, g->unknown, ctx->stream));
   g->sync();
+  return g.release();
+}
+
+// Host images of a job's graph arrays for a host-built graph under `cc`,
+// in the order of arrays(): edge lists as chunk chains in their insertion
+// order. Ranks are written when `rank_of` / `order` are given (else 0).
+struct GraphImage {
+  std::vector<std::vector<char>> bufs;
+  int32_t n_nodes = 0, n_chunks = 0, n_edges = 0, n_paths = 0, path_used = 0, n_rank = 0;
+};
+
+int64_t build_chunks(const BuildGraph &bg) {
+  int64_t chunks = 0;
+  for (int64_t i = 0; i < bg.n(); ++i)
+    chunks += (int64_t(bg.in_id[size_t(i)].size()) + CHUNK - 1) / CHUNK +
+              (int64_t(bg.out_id[size_t(i)].size()) + CHUNK - 1) / CHUNK;
+  return chunks;
+}
+
+int64_t build_path_items(const BuildGraph &bg) {
+  int64_t items = 0;
+  for (auto &pth : bg.paths) items += int64_t(pth.size());
+  return items;
+}
+
+GraphImage graph_image(const BuildGraph &bg, const Caps &cc, const std::vector<int32_t> *rank_of,
+                       const std::vector<int32_t> *order) {
+  const int64_t n = bg.n();
+  const int sg = cc.sigma;
+  const size_t N = size_t(cc.node_cap);
+  std::vector<uint8_t> base(N, 0);
+  std::vector<int32_t> parent(N, 0), rank(N, 0), cov(N, 0), ih(N, -1), it(N, -1), ic(N, 0), oh(N, -1), ot(N, -1),
+      oc(N, 0), r2n(N, 0), al(N * size_t(sg), -1);
+  std::vector<int32_t> cid(size_t(cc.chunk_cap) * CHUNK, 0), cw(size_t(cc.chunk_cap) * CHUNK, 0),
+      cnext(size_t(cc.chunk_cap), -1);
+  std::vector<int32_t> pit(size_t(cc.path_cap) + 1, 0), poff(size_t(cc.max_paths) + 1, 0),
+      pseq(size_t(cc.max_paths) + 1, 0);
+  int32_t nch = 0;
+  auto put_list = [&](const std::vector<int32_t> &ids, const std::vector<int32_t> &ws, int32_t &head, int32_t &tail,
+                      int32_t &cnt) {
+    cnt = int32_t(ids.size());
+    int32_t prev = -1;
+    for (size_t k = 0; k < ids.size(); ++k) {
+      if (k % CHUNK == 0) {
+        const int32_t ch = nch++;
+        if (prev < 0)
+          head = ch;
+        else
+          cnext[size_t(prev)] = ch;
+        prev = ch;
+        tail = ch;
+      }
+      cid[size_t(prev) * CHUNK + k % CHUNK] = ids[k];
+      cw[size_t(prev) * CHUNK + k % CHUNK] = ws[k];
+    }
+  };
+  for (int64_t i = 0; i < n; ++i) {
+    const size_t u = size_t(i);
+    base[u] = uint8_t(bg.base[u]);
+    parent[u] = bg.parent[u];
+    cov[u] = bg.coverage[u];
+    for (int k = 0; k < sg; ++k) al[u * size_t(sg) + size_t(k)] = bg.aligned[u * size_t(sg) + size_t(k)];
+    put_list(bg.in_id[u], bg.in_w[u], ih[u], it[u], ic[u]);
+    put_list(bg.out_id[u], bg.out_w[u], oh[u], ot[u], oc[u]);
+    if (rank_of) rank[u] = (*rank_of)[u];
+  }
+  if (order)
+    for (size_t r = 0; r < order->size(); ++r) r2n[r] = (*order)[r];
+  int32_t used = 0;
+  for (size_t k = 0; k < bg.paths.size(); ++k) {
+    poff[k] = used;
+    pseq[k] = bg.path_seq[k];
+    for (int32_t id : bg.paths[k]) pit[size_t(used++)] = id;
+  }
+  poff[bg.paths.size()] = used;
+  GraphImage img;
+  auto add = [&](const void *p, size_t bytes) {
+    img.bufs.emplace_back(reinterpret_cast<const char *>(p), reinterpret_cast<const char *>(p) + bytes);
+  };
+  add(base.data(), N);
+  for (auto *v : {&parent, &rank, &cov, &ih, &it, &ic, &oh, &ot, &oc, &r2n}) add(v->data(), N * 4);
+  add(al.data(), al.size() * 4);
+  add(cid.data(), cid.size() * 4);
+  add(cw.data(), cw.size() * 4);
+  add(cnext.data(), cnext.size() * 4);
+  add(pit.data(), size_t(cc.path_cap) * 4 + 4);
+  add(poff.data(), size_t(cc.max_paths + 1) * 4);
+  add(pseq.data(), size_t(cc.max_paths) * 4 + 4);
+  img.n_nodes = int32_t(n);
+  img.n_chunks = nch;
+  img.n_edges = int32_t(bg.edges());
+  img.n_paths = int32_t(bg.paths.size());
+  img.path_used = used;
+  img.n_rank = order ? int32_t(order->size()) : 0;
+  return img;
+}
+
+// Copies a graph image into a laid-out job's arrays and sets its counts.
+void put_image(const GraphImage &img, const Caps &cc, Job &J, cudaStream_t stream) {
+  const auto dst = arrays(J, cc);
+  for (size_t k = 0; k < dst.size(); ++k)
+    CK(cudaMemcpyAsync(dst[k].first, img.bufs[k].data(), std::min(dst[k].second, img.bufs[k].size()),
+                       cudaMemcpyHostToDevice, stream));
+  J.n_nodes = img.n_nodes;
+  J.n_chunks = img.n_chunks;
+  J.n_edges = img.n_edges;
+  J.n_paths = img.n_paths;
+  J.path_used = img.path_used;
+  J.n_rank = img.n_rank;
+}
+
+// A device graph from a host-built one (GFA input), ranked by the device's
+// LIFO toposort (which rejects cycles). Room is left for `reserve` more
+// nodes; the graph grows on demand when reads extend it.
+poa_graph *import_graph(poa_ctx *ctx, const HostParams &hp, const BuildGraph &bg, int64_t reserve) {
+  const int64_t n = bg.n(), chunks = build_chunks(bg), items = build_path_items(bg);
+  if (n + reserve > INT32_MAX / 4 || 2 * chunks + reserve > INT32_MAX / 4)
+    throw AlignError{POA_ERR_INVALID, "graph is too large"};
+  Caps c;
+  c.node_cap = int32_t(n + reserve + 8);
+  c.chunk_cap = int32_t(chunks + 2 * reserve + 16);
+  c.path_cap = int32_t(items + reserve + 8);
+  c.max_paths = int32_t(bg.paths.size() + 8);
+  std::unique_ptr<poa_graph> g(new_graph(ctx, hp, c));
+  const GraphImage img = graph_image(bg, g->caps, nullptr, nullptr);
+  put_image(img, g->caps, g->h, ctx->stream);
+  g->h.status = ST_OK;
+  g->upload();  // synchronises: the image is copied before it goes out of scope
+  g->sync();
+  ctx->ensure_arena(std::max<int64_t>(int64_t(g->h.n_nodes) * 8 + 64, int64_t(1) << 20));
+  CK(launch_toposort(g->d_job, ctx->arena, ctx->arena_bytes, ctx->stream));
+  g->check_status();
   return g.release();
 }
 
@@ -945,6 +1081,31 @@ int poa_graph_new(poa_ctx *ctx, const poa_params *params, poa_graph **out) {
 
 void poa_graph_free(poa_graph *graph) { delete graph; }
 
+int poa_graph_read_gfa(poa_ctx *ctx, const poa_params *params, const char *text, int64_t len, poa_graph **out,
+                       char **records, int64_t *records_len) {
+  *out = nullptr;
+  *records = nullptr;
+  *records_len = 0;
+  return api(ctx, [&] {
+    HostParams hp = checked_params(params);
+    if (len < 0 || (len > 0 && !text)) throw AlignError{POA_ERR_INVALID, "invalid GFA text"};
+    std::vector<GfaRecord> recs;
+    BuildGraph bg = [&] {
+      try {
+        return read_gfa(hp, text, size_t(len), recs);
+      } catch (const std::runtime_error &e) {
+        throw AlignError{POA_ERR_ALIGN, e.what()};
+      }
+    }();
+    std::unique_ptr<poa_graph> g(import_graph(ctx, hp, bg, 1024));
+    std::string r;
+    for (auto &x : recs) r += x.name + "\t" + x.seq + "\n";
+    *records = dup_string(r);
+    *records_len = int64_t(r.size());
+    *out = g.release();
+  });
+}
+
 int poa_align_sequences(poa_ctx *ctx, const poa_params *params, int64_t n_seqs, const uint8_t *const *seqs,
                         const int64_t *lens, poa_graph **out) {
   *out = nullptr;
@@ -989,6 +1150,7 @@ int poa_align(poa_ctx *ctx, const poa_params *params, poa_graph *graph, const ui
   *out_len = 0;
   return api(ctx, [&] {
     HostParams hp = checked_params(params);
+    if (!graph || graph->ctx != ctx) throw AlignError{POA_ERR_INVALID, "the graph belongs to another context"};
     if (len < 0 || len > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
     auto v = hp.seeding ? seeded_align(ctx, hp, graph, query, len)
                         : align_path(ctx, hp, graph, query, len, 0, 0, 1, 0, hp.b, 0, 1);
@@ -1615,6 +1777,12 @@ struct ServerJob {
   int64_t id = 0;
   std::vector<uint8_t> bytes;  // the reads, back to back
   std::vector<int64_t> lens;
+  // an initial graph to extend (GFA jobs): built and ranked on the host at
+  // submission, copied into the job's storage at admission; the job's reads
+  // get sequence ids after its `existing` path records
+  std::unique_ptr<BuildGraph> init;
+  std::vector<int32_t> init_rank, init_order;
+  int32_t existing = 0;
   Caps caps;
   uint64_t storage_bytes = 0, reads_bytes = 0, arena_bytes = 0;
   char *storage = nullptr, *reads = nullptr, *arena = nullptr;
@@ -1694,6 +1862,12 @@ struct poa_server {
     c.chunk_cap = int32_t(std::min<int64_t>(2 * (sum + 3 * k) + 16, INT32_MAX / 2));
     c.path_cap = int32_t(std::min<int64_t>(sum + k + 1, INT32_MAX / 2));
     c.max_paths = int32_t(k + 1);
+    if (sj.init) {
+      c.node_cap = int32_t(std::min<int64_t>(int64_t(c.node_cap) + sj.init->n(), INT32_MAX / 2));
+      c.chunk_cap = int32_t(std::min<int64_t>(int64_t(c.chunk_cap) + build_chunks(*sj.init), INT32_MAX / 2));
+      c.path_cap = int32_t(std::min<int64_t>(int64_t(c.path_cap) + build_path_items(*sj.init), INT32_MAX / 2));
+      c.max_paths = int32_t(std::min<int64_t>(int64_t(c.max_paths) + int64_t(sj.init->paths.size()), INT32_MAX / 2));
+    }
     sj.caps = c;
     Job J{};
     sj.storage_bytes = layout(c, nullptr, &J) + 256;
@@ -1707,7 +1881,7 @@ struct poa_server {
     for (int64_t l : sj.lens) mx = std::max(mx, l);
     const double band = std::min(2.0 * (double(hp.b) + (hp.f ? double(mx) / double(hp.f) : double(mx))) + 16.0,
                                  double(mx) + 16.0);
-    const double rows = double(mx) * (1.0 + 0.1 * double(sj.lens.size())) + 16.0;
+    const double rows = double(mx) * (1.0 + 0.1 * double(sj.lens.size())) + 16.0 + (sj.init ? sj.init->n() : 0);
     return uint64_t(arena_scale * rows * (band * 12.0 + 400.0)) + (uint64_t(1) << 20);
   }
 
@@ -1841,8 +2015,11 @@ bool poa_server::launch_wave() {
     w.stream = free_streams.back();
     free_streams.pop_back();
   }
-  // fresh jobs first (they are reset to Graph::new), parked ones keep their graph
+  // fresh jobs without an initial graph first (they are reset to
+  // Graph::new), then fresh jobs with one (their graph is copied in), then
+  // parked ones, which keep their graph
   std::stable_partition(adm.begin(), adm.end(), [](const ServerJob *j) { return j->fresh; });
+  std::stable_partition(adm.begin(), adm.end(), [](const ServerJob *j) { return j->fresh && !j->init; });
   const cudaStream_t stream = streams[size_t(w.stream)];
   const double t = now_s();
   std::vector<Job> hj(adm.size());
@@ -1850,9 +2027,17 @@ bool poa_server::launch_wave() {
   for (size_t k = 0; k < adm.size(); ++k) {
     ServerJob &sj = *adm[k];
     if (sj.fresh) {
-      ++n_fresh;
+      if (!sj.init) ++n_fresh;
       Job J{};
       layout(sj.caps, sj.storage, &J);
+      if (sj.init) {
+        // the initial graph, ranked in the reference's LIFO order
+        const GraphImage img = graph_image(*sj.init, sj.caps, &sj.init_rank, &sj.init_order);
+        put_image(img, sj.caps, J, stream);
+        CK(cudaStreamSynchronize(stream));  // the image goes out of scope
+        J.order_exact = 1;
+        J.seq_base = sj.existing;
+      }
       const int64_t n = int64_t(sj.lens.size());
       J.read_off = reinterpret_cast<int64_t *>(sj.reads);
       J.read_len = reinterpret_cast<int32_t *>(sj.reads + n * 8);
@@ -2000,6 +2185,47 @@ int poa_server_submit(poa_ctx *ctx, poa_server *sv, int64_t n_seqs, const uint8_
   if (!ctx || !sv || !job_id || (n_seqs > 0 && (!seqs || !lens)) || n_seqs < 0) return POA_ERR_INVALID;
   return api(ctx, [&] {
     auto sj = std::make_unique<ServerJob>();
+    int64_t total = 0;
+    for (int64_t r = 0; r < n_seqs; ++r) {
+      if (lens[r] < 0 || lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
+      total += lens[r];
+    }
+    sj->bytes.resize(size_t(total));
+    sj->lens.assign(lens, lens + n_seqs);
+    int64_t at = 0;
+    for (int64_t r = 0; r < n_seqs; ++r) {
+      if (lens[r]) std::memcpy(sj->bytes.data() + at, seqs[r], size_t(lens[r]));
+      at += lens[r];
+    }
+    poa_server::size_job(*sj, int(sv->hp.alphabet.size()));
+    sj->arena_bytes = sv->first_arena(*sj);
+    sj->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!sv->fatal.empty()) throw AlignError{POA_ERR_CUDA, sv->fatal};
+    sj->id = sv->next_id++;
+    *job_id = sj->id;
+    if (sv->first_submit < 0) sv->first_submit = sj->t_submit;
+    sv->pending.push_back(sj->id);
+    sv->jobs[sj->id] = std::move(sj);
+    sv->cv.notify_all();
+  });
+}
+
+int poa_server_submit_gfa(poa_ctx *ctx, poa_server *sv, const char *gfa, int64_t gfa_len, int64_t n_seqs,
+                          const uint8_t *const *seqs, const int64_t *lens, int64_t *job_id) {
+  if (!ctx || !sv || !job_id || (n_seqs > 0 && (!seqs || !lens)) || n_seqs < 0 || gfa_len < 0 ||
+      (gfa_len > 0 && !gfa))
+    return POA_ERR_INVALID;
+  return api(ctx, [&] {
+    auto sj = std::make_unique<ServerJob>();
+    std::vector<GfaRecord> recs;
+    try {
+      sj->init.reset(new BuildGraph(read_gfa(sv->hp, gfa, size_t(gfa_len), recs)));
+      sj->init->toposort(sj->init_rank, sj->init_order);
+    } catch (const std::runtime_error &e) {
+      throw AlignError{POA_ERR_ALIGN, e.what()};
+    }
+    sj->existing = int32_t(recs.size());
     int64_t total = 0;
     for (int64_t r = 0; r < n_seqs; ++r) {
       if (lens[r] < 0 || lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
@@ -2177,6 +2403,7 @@ namespace poa {
 
 Job *graph_device_job(poa_graph *g) { return g->d_job; }
 int graph_alphabet(const poa_graph *g) { return g->sigma; }
+const poa_ctx *graph_context(const poa_graph *g) { return g->ctx; }
 cudaStream_t ctx_stream(const poa_ctx *c) { return c->stream; }
 int ctx_device(const poa_ctx *c) { return c->device; }
 void ctx_set_error(poa_ctx *c, const std::string &msg) {

@@ -320,6 +320,7 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   add_node(J, sigma, unknown);
   add_node(J, sigma, unknown);
   J->next_read = 0;
+  J->seq_base = 0;
   J->status = ST_OK;
   J->err_i = J->err_j = 0;
   J->n_items = 0;

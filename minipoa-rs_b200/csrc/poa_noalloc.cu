@@ -29,6 +29,7 @@ namespace poa {
 // Defined in poa_host.cu.
 Job *graph_device_job(poa_graph *g);
 int graph_alphabet(const poa_graph *g);
+const poa_ctx *graph_context(const poa_graph *g);
 cudaStream_t ctx_stream(const poa_ctx *c);
 int ctx_device(const poa_ctx *c);
 void ctx_set_error(poa_ctx *c, const std::string &msg);
@@ -80,14 +81,17 @@ __device__ __forceinline__ WarpSmem *noalloc_warp_smem() {
 
 // align::align (align.rs:81-188) of one query, one warp, scratch in `arena`;
 // the path goes to the caller's device buffer as AlignedBase records.
+// A path longer than the caller's buffer (out_cap items) is not written and
+// ends the call with ST_OUT_TOO_SMALL.
 __global__ void k_align_noalloc(Job *J, DevParams P, char *arena, int64_t bytes, const uint8_t *q, int qlen,
-                                poa_aligned_base *out, int64_t *out_n) {
+                                poa_aligned_base *out, int64_t out_cap, int64_t *out_n) {
   const int lane = threadIdx.x & 31;
   Scratch s;
   int n_items = 0;
   Work cells{};
   ring_default(noalloc_warp_smem());
-  const int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, noalloc_warp_smem());
+  int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, noalloc_warp_smem());
+  if (st == ST_OK && int64_t(n_items) > out_cap) st = ST_OUT_TOO_SMALL;
   if (st == ST_OK) {
     for (int k = lane; k < n_items; k += 32) {
       const int4 it = s.items[k];
@@ -122,6 +126,7 @@ extern "C" int poa_align_noalloc(poa_ctx *ctx, const poa_params *params, poa_gra
   };
   if (!params || !graph || !d_out || !d_out_len || (len > 0 && !d_query))
     return fail(POA_ERR_INVALID, "null argument");
+  if (graph_context(graph) != ctx) return fail(POA_ERR_INVALID, "the graph belongs to another context");
   const HostParams hp = HostParams::from(params);
   const std::string bad = hp.validate();
   if (!bad.empty()) return fail(POA_ERR_INVALID, bad);
@@ -171,7 +176,7 @@ extern "C" int poa_align_noalloc(poa_ctx *ctx, const poa_params *params, poa_gra
   P.largest = hp.largest();
   k_align_noalloc<<<1, 32, sizeof(WarpSmem), stream>>>(graph_device_job(graph), P,
                                                         reinterpret_cast<char *>(base + kArenaOffset), arena_bytes,
-                                                        d_query, int(len), d_out, d_out_len);
+                                                        d_query, int(len), d_out, out_cap, d_out_len);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(POA_ERR_CUDA, cudaGetErrorString(e));
   if (!graph_read_job(graph, &h, &err)) return fail(POA_ERR_CUDA, err);

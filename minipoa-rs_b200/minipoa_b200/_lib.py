@@ -78,6 +78,7 @@ SIGNATURES = {
     "poa_params_validate": (ctypes.c_int, [_vp, _cp]),
     "poa_graph_new": (ctypes.c_int, [_vp, _cp, P(_vp)]),
     "poa_graph_free": (None, [_vp]),
+    "poa_graph_read_gfa": (ctypes.c_int, [_vp, _cp, ctypes.c_char_p, _i64, P(_vp), P(_vp), P(_i64)]),
     "poa_align_sequences": (ctypes.c_int, [_vp, _cp, _i64, P(_u8p), P(_i64), P(_vp)]),
     "poa_extend_graph": (ctypes.c_int, [_vp, _cp, _vp, _i64, P(_u8p), P(_i64), _i64]),
     "poa_align": (ctypes.c_int, [_vp, _cp, _vp, _u8p, _i64, P(P(AlignedBaseC)), P(_i64)]),
@@ -105,6 +106,7 @@ SIGNATURES = {
     "poa_batch_transfer_bytes": (ctypes.c_int, [_vp, _vp, P(_u64), P(_u64)]),
     "poa_server_create": (ctypes.c_int, [_vp, _cp, _u64, _i32, P(_vp)]),
     "poa_server_submit": (ctypes.c_int, [_vp, _vp, _i64, P(_u8p), P(_i64), P(_i64)]),
+    "poa_server_submit_gfa": (ctypes.c_int, [_vp, _vp, ctypes.c_char_p, _i64, _i64, P(_u8p), P(_i64), P(_i64)]),
     "poa_server_wait": (ctypes.c_int, [_vp, _vp, _i64, ctypes.c_double, P(_i32)]),
     "poa_server_job_info": (ctypes.c_int, [_vp, _vp, _i64, P(ServerJobInfo)]),
     "poa_server_output": (ctypes.c_int, [_vp, _vp, _i64, _i32, _ccp, _ccp, P(ctypes.c_char_p), P(_i64)]),

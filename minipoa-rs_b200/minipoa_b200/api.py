@@ -284,14 +284,42 @@ def extend_graph(params: Params, graph: Graph, sequences: Seq, existing: int) ->
     graph.ctx.check(graph.L.poa_extend_graph(graph.ctx.h, ctypes.byref(c), graph.h, len(raw), arr, lens, existing))
 
 
-def run(params: Params, sequences: Seq[Sequence], ctx: Optional[Context] = None) -> str:
-    """lib.rs:207-242 after input parsing: RNA detection, the read loop and
-    the selected output (params.result: 0 consensus, 1 MSA, 2 GFA)."""
+def read_gfa(params: Params, text, ctx: Optional[Context] = None) -> Tuple["Graph", List[Sequence]]:
+    """io::read_gfa (called at lib.rs:214-218): GFA text -> (graph resident on
+    the device, the path records in file order)."""
+    ctx = ctx or default_context()
+    c, keep = params.to_c()
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    h = ctypes.c_void_p()
+    recs = ctypes.c_void_p()
+    n = ctypes.c_int64()
+    ctx.check(ctx.L.poa_graph_read_gfa(ctx.h, ctypes.byref(c), b, len(b), ctypes.byref(h), ctypes.byref(recs),
+                                       ctypes.byref(n)))
+    raw = ctypes.string_at(recs, n.value).decode()
+    ctx.L.poa_free(recs)
+    records = []
+    for line in raw.splitlines():
+        name, seq = line.split("\t", 1)
+        records.append(Sequence(name=name, seq=seq.encode()))
+    return Graph(ctx=ctx, handle=h), records
+
+
+def run(params: Params, sequences: Seq[Sequence], ctx: Optional[Context] = None, incremental=None) -> str:
+    """lib.rs:207-242 after input parsing: the optional initial GFA graph
+    (`incremental`, GFA text; its path records come first and progressive
+    ordering is off), RNA detection, the read loop and the selected output
+    (params.result: 0 consensus, 1 MSA, 2 GFA)."""
+    params = params.copy()
+    if incremental is not None:
+        g, records = read_gfa(params, incremental, ctx)
+        sequences = records + list(sequences)
     if not sequences:
         raise PoaError(_lib.POA_ERR_INVALID, "input contains no sequences")
-    params = params.copy()
     params.is_rna = len(params.alphabet) <= 5 and any(b"U" in s.seq.upper() for s in sequences)
-    g = align_sequences(params, sequences, ctx)
+    if incremental is not None:
+        extend_graph(params.copy(progressive=False), g, sequences, len(records))
+    else:
+        g = align_sequences(params, sequences, ctx)
     if params.result == 0:
         return ">consensus sequence\n" + g.consensus(params)[0].decode() + "\n"
     if params.result == 1:
@@ -408,10 +436,18 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, reads: Seq[bytes]) -> int:
+    def submit(self, reads: Seq[bytes], gfa=None) -> int:
+        """Queues a job: its reads, optionally extending an initial graph given
+        as GFA text (the -i workflow; the reads' sequence ids follow the GFA's
+        path records)."""
         arr, lens, _bufs = _seq_arrays([_bytes(r) for r in reads])
         job = ctypes.c_int64()
-        self.ctx.check(self.L.poa_server_submit(self.ctx.h, self.h, len(reads), arr, lens, ctypes.byref(job)))
+        if gfa is None:
+            self.ctx.check(self.L.poa_server_submit(self.ctx.h, self.h, len(reads), arr, lens, ctypes.byref(job)))
+        else:
+            g = gfa.encode() if isinstance(gfa, str) else bytes(gfa)
+            self.ctx.check(self.L.poa_server_submit_gfa(self.ctx.h, self.h, g, len(g), len(reads), arr, lens,
+                                                        ctypes.byref(job)))
         return job.value
 
     def wait(self, job: int, timeout_ms: float = -1.0) -> int:

@@ -85,3 +85,46 @@ def seeded_window_set(seed: int = 1002) -> List[bytes]:
     """16,500 bp ancestor, 100 reads at ~5% error (3% substitution, 1%
     insertion, 1% deletion, indel lengths geometric with mean 1.5)."""
     return read_set(np.random.default_rng(seed), 16500, 100, 0.03, 0.01, 0.01, indel_mean=1.5)
+
+
+PROTEIN_ALPHABET = b"ACDEFGHIKLMNPQRSTVWYX"
+
+
+def protein_matrix(seed: int = 1004) -> List[int]:
+    """Symmetric 20 x 20 integer matrix (diagonal uniform in 4..11,
+    off-diagonal uniform in -4..2) plus a last (X) row and column of 0 with
+    X-X = 5, in the layout of a matrix file over PROTEIN_ALPHABET."""
+    rng = np.random.default_rng(seed)
+    k = len(PROTEIN_ALPHABET)
+    m = [0] * (k * k)
+    for i in range(k - 1):
+        for j in range(i, k - 1):
+            v = int(rng.integers(4, 12)) if i == j else int(rng.integers(-4, 3))
+            m[i * k + j] = m[j * k + i] = v
+    m[k * k - 1] = 5
+    return m
+
+
+def protein_families(n_families: int = 1000, depth: int = 30, seed: int = 1004) -> List[List[bytes]]:
+    """Protein families: a uniform random ancestor of length uniform in
+    300..800 over 20 amino acids and `depth` members at 20% divergence (15%
+    substitution, 2.5% deletion, 2.5% insertion per ancestor residue)."""
+    rng = np.random.default_rng(seed + 1)
+    fams = []
+    for _ in range(n_families):
+        L = int(rng.integers(300, 801))
+        anc = rng.integers(0, 20, size=L)
+        fam = []
+        for _ in range(depth):
+            u = rng.random(L)
+            keep = u >= 0.025
+            sub = (rng.random(L) < 0.15) & keep
+            res = np.where(sub, rng.integers(0, 20, size=L), anc)[keep]
+            ins = rng.random(res.shape[0]) < 0.025
+            if ins.any():
+                pos = np.flatnonzero(ins)
+                res = np.insert(res, pos + 1, rng.integers(0, 20, size=pos.shape[0]))
+            fam.append(bytes(PROTEIN_ALPHABET[int(x)] for x in res))
+        fams.append(fam)
+    return fams
+

@@ -130,6 +130,8 @@ int orc_batch_run(const orc_params *p, int64_t n_sets, const int64_t *set_off, c
 /* Test hooks for the AVX2 insertion-prefix scan (align.rs:459-491). */
 int orc_avx2_available(void);
 uint64_t orc_fnv1a(const uint8_t *data, int64_t len);
+int orc_read_gfa(const orc_params *p, const char *text, int64_t len, void **out_graph, char **records,
+                 int64_t *records_len);
 void orc_avx2_prefix(const int32_t *md8, int32_t carry, int32_t open, int32_t ext, int32_t *out8);
 
 #ifdef __cplusplus

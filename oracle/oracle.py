@@ -100,6 +100,7 @@ def lib():
                                     ctypes.c_int, P(u64), P(u64)]
         L.orc_avx2_prefix.argtypes = [P(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                       P(ctypes.c_int32)]
+        L.orc_read_gfa.argtypes = [cp, ctypes.c_char_p, i64, P(vp), P(ctypes.c_void_p), P(i64)]
         L.orc_fnv1a.argtypes = [ctypes.c_char_p, i64]
         L.orc_fnv1a.restype = u64
         _lib = L
@@ -359,3 +360,18 @@ def fnv1a(data) -> int:
     """FNV-1a of a text or byte string, the hash batch_run reports per set."""
     b = data.encode() if isinstance(data, str) else bytes(data)
     return lib().orc_fnv1a(b, len(b))
+
+
+def read_gfa(params, text):
+    """GFA text -> (OracleGraph, [(name, sequence)]) (io::read_gfa as restated
+    in poa_oracle.cpp from the reference's tests)."""
+    c, keep = _params(params)
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    h = ctypes.c_void_p()
+    recs = ctypes.c_void_p()
+    n = ctypes.c_int64()
+    _check(lib().orc_read_gfa(ctypes.byref(c), b, len(b), ctypes.byref(h), ctypes.byref(recs), ctypes.byref(n)))
+    raw = ctypes.string_at(recs, n.value).decode()
+    lib().orc_free(recs)
+    records = [tuple(line.split("\t", 1)) for line in raw.splitlines()]
+    return OracleGraph(params, handle=h.value), [(nm, sq.encode()) for nm, sq in records]

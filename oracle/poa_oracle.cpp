@@ -14,6 +14,7 @@
 #include <immintrin.h>
 
 #include <algorithm>
+#include <map>
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
@@ -1048,6 +1049,130 @@ static void extend_graph(const Params &params, Graph &graph, usize n, const uint
   }
 }
 
+// GFA input. The reference's reader (io::read_gfa, declared by src/lib.rs:7
+// and called at lib.rs:214-218) is absent from its source tree (src/io.rs is
+// missing), so this restates the behaviour its tests pin:
+// tests/io_cli.rs:375-399 (multi-base segments, paths become records and
+// graph paths, round trip through Graph::gfa), :401-408 (links without
+// paths still build a graph), :410-431 (rejected inputs: duplicate
+// segments, unknown references, reverse orientations, self links, cycles,
+// non-zero overlaps, segments without sequence), :564-581 (extension of a
+// GFA graph), :584-610 (empty paths; a path revisiting a node fails with
+// "revisits"). The construction order, which edge weights and tie-breaks
+// depend on: nodes per segment base in S-line order; then each path in
+// P-line order through add_path from the source; then the segment-internal
+// and L-line edges that no path created (add_edge, weight 1); then edges
+// from the source to every node without an incoming edge and from every
+// node without an outgoing edge to the sink (node order); then the LIFO
+// toposort (graph.rs:125-178), which rejects cycles.
+struct Record {
+  std::string name, comment, seq;
+};
+
+static std::vector<std::string> split(const std::string &s, char sep) {
+  std::vector<std::string> out;
+  size_t a = 0;
+  for (;;) {
+    const size_t b = s.find(sep, a);
+    out.push_back(s.substr(a, b == std::string::npos ? std::string::npos : b - a));
+    if (b == std::string::npos) break;
+    a = b + 1;
+  }
+  return out;
+}
+
+static Graph read_gfa(const Params &p, const std::string &text, std::vector<Record> &recs) {
+  struct Link {
+    std::string from, to;
+  };
+  struct PathLine {
+    std::string name;
+    std::vector<std::string> segs;
+  };
+  std::vector<std::string> seg_names, seg_seqs;
+  std::map<std::string, usize> seg_index;
+  std::vector<Link> links;
+  std::vector<PathLine> plines;
+  for (std::string line : split(text, '\n')) {
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    if (line.empty() || line[0] == '#') continue;
+    const auto f = split(line, '\t');
+    if (f[0] == "S") {
+      if (f.size() < 3) throw Error("malformed GFA segment line");
+      if (f[2].empty() || f[2] == "*") throw Error("GFA segment " + f[1] + " has no sequence");
+      if (seg_index.count(f[1])) throw Error("duplicate GFA segment " + f[1]);
+      seg_index[f[1]] = seg_names.size();
+      seg_names.push_back(f[1]);
+      seg_seqs.push_back(f[2]);
+    } else if (f[0] == "L") {
+      if (f.size() < 6) throw Error("malformed GFA link line");
+      if (f[2] != "+" || f[4] != "+") throw Error("unsupported GFA link orientation");
+      if (f[5] != "0M" && f[5] != "*") throw Error("unsupported GFA link overlap " + f[5]);
+      links.push_back({f[1], f[3]});
+    } else if (f[0] == "P") {
+      if (f.size() < 3) throw Error("malformed GFA path line");
+      PathLine pl{f[1], {}};
+      if (f[2] != "*") {
+        for (const auto &e : split(f[2], ',')) {
+          if (e.size() < 2) throw Error("malformed GFA path " + f[1]);
+          if (e.back() == '-') throw Error("unsupported GFA path orientation in " + f[1]);
+          if (e.back() != '+') throw Error("malformed GFA path " + f[1]);
+          pl.segs.push_back(e.substr(0, e.size() - 1));
+        }
+      }
+      plines.push_back(std::move(pl));
+    }
+  }
+  Graph g(p);
+  std::vector<std::vector<usize>> seg_nodes(seg_names.size());
+  for (usize k = 0; k < seg_names.size(); ++k)
+    for (char c : seg_seqs[k]) seg_nodes[k].push_back(g.add_node(p.encode(uint8_t(c))));
+  auto seg_of = [&](const std::string &name, const std::string &what) -> usize {
+    auto it = seg_index.find(name);
+    if (it == seg_index.end()) throw Error("GFA " + what + " references unknown segment " + name);
+    return it->second;
+  };
+  std::vector<std::pair<usize, usize>> link_nodes;
+  for (const auto &l : links) {
+    const usize a = seg_of(l.from, "link"), b = seg_of(l.to, "link");
+    if (a == b) throw Error("GFA link from segment " + l.from + " to itself forms a cycle");
+    link_nodes.push_back({seg_nodes[a].back(), seg_nodes[b].front()});
+  }
+  recs.clear();
+  for (usize k = 0; k < plines.size(); ++k) {
+    const auto &pl = plines[k];
+    std::vector<AlignedBase> items{{0, g.nodes[0].base, NONE}};
+    std::vector<char> seen(g.nodes.size(), 0);
+    std::string seq;
+    for (const auto &sn : pl.segs) {
+      const usize sg = seg_of(sn, "path " + pl.name);
+      for (usize id : seg_nodes[sg]) {
+        if (seen[id]) throw Error("GFA path " + pl.name + " revisits segment " + sn);
+        seen[id] = 1;
+        items.push_back({i64(id), g.nodes[id].base, NONE});
+      }
+      seq += seg_seqs[sg];
+    }
+    g.add_path(k, items);
+    recs.push_back({pl.name, "", seq});
+  }
+  auto has_edge = [&](usize a, usize b) {
+    const auto &out = g.nodes[a].outgoing;
+    return std::find(out.begin(), out.end(), b) != out.end();
+  };
+  for (const auto &nodes : seg_nodes)
+    for (usize k = 1; k < nodes.size(); ++k)
+      if (!has_edge(nodes[k - 1], nodes[k])) g.add_edge(nodes[k - 1], nodes[k]);
+  for (const auto &ln : link_nodes)
+    if (!has_edge(ln.first, ln.second)) g.add_edge(ln.first, ln.second);
+  for (usize id = 2; id < g.nodes.size(); ++id)
+    if (g.nodes[id].incoming.empty()) g.add_edge(0, id);
+  for (usize id = 2; id < g.nodes.size(); ++id)
+    if (g.nodes[id].outgoing.empty()) g.add_edge(id, 1);
+  g.toposort(false);
+  return g;
+}
+
 }  // namespace orc
 
 // ---------------------------------------------------------------------------
@@ -1347,6 +1472,26 @@ __attribute__((target("avx2"))) void orc_avx2_prefix(const int32_t *md8, int32_t
                                                      int32_t *out8) {
   __m256i v = insertion_prefix(_mm256_loadu_si256((const __m256i *)md8), carry, open, ext);
   _mm256_storeu_si256((__m256i *)out8, v);
+}
+
+// GFA text -> graph (io::read_gfa as restated above). Records come back as
+// "name\tsequence\n" lines.
+int orc_read_gfa(const orc_params *p, const char *text, int64_t len, void **out_graph, char **records,
+                 int64_t *records_len) {
+  *out_graph = nullptr;
+  *records = nullptr;
+  *records_len = 0;
+  return guard([&] {
+    Params pp = Params::from(p);
+    pp.validate();
+    std::vector<Record> recs;
+    auto *g = new Graph(read_gfa(pp, std::string(text, size_t(len)), recs));
+    std::string r;
+    for (auto &x : recs) r += x.name + "\t" + x.seq + "\n";
+    *records = str_out(r);
+    *records_len = int64_t(r.size());
+    *out_graph = g;
+  });
 }
 
 }  // extern "C"

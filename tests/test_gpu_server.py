@@ -124,3 +124,36 @@ def test_server_refuses_a_job_larger_than_its_pool(mp):
     small = server.submit([b"ACGTACGT", b"ACGAACGT"])
     assert server.wait(small) == mp._lib.POA_SERVER_DONE
     server.close()
+
+
+def test_server_extends_gfa_graphs_like_the_oracle(mp, oracle):
+    # serving jobs that bring an initial graph (GFA of prior reads) and new
+    # reads, mixed with plain jobs: each result equals the oracle's read_gfa +
+    # extend_graph (the -i workflow, src/lib.rs:214-231)
+    params = Params()
+    rng = np.random.default_rng(606)
+    server = mp.Server(params)
+    cases = []
+    for k in range(6):
+        reads = rc.synthetic_reads(rng, int(rng.integers(200, 700)), int(rng.integers(12, 30)), 0.05, 0.015, 0.015)
+        n_prior = int(rng.integers(4, 10))
+        prior, new = reads[:n_prior], reads[n_prior:]
+        names = [Sequence(name=f"p{i}", seq=s) for i, s in enumerate(prior)]
+        gfa = oracle.align_sequences(params, prior).gfa(params, names)
+        cases.append((gfa, names, new))
+    plain = _jobs(9, 6, 150, 600, 3, 8)
+    ids = []
+    for k in range(6):
+        ids.append(server.submit(cases[k][2], gfa=cases[k][0]))
+        server.submit(plain[k])
+    for k, (gfa, names, new) in enumerate(cases):
+        assert server.wait(ids[k]) == mp._lib.POA_SERVER_DONE
+        o, orecs = oracle.read_gfa(params, gfa)
+        allrecs = names + [Sequence(name=f"n{i}", seq=s) for i, s in enumerate(new)]
+        oracle.extend_graph(params, o, [r.seq for r in allrecs], len(orecs))
+        assert server.output(ids[k], 1, allrecs) == o.msa(params, allrecs)
+        assert server.output(ids[k], 2, allrecs) == o.gfa(params, allrecs)
+        assert server.output(ids[k], 0) == ">consensus sequence\n" + o.consensus(params)[0].decode() + "\n"
+    with pytest.raises(mp.PoaError, match="revisits"):
+        server.submit([b"ACGT"], gfa="S\ta\tA\nP\tc\ta+,a+\t*\n")
+    server.close()

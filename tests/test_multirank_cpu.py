@@ -67,3 +67,60 @@ def test_single_process_needs_no_process_group(monkeypatch):
     world, rank, _, pg = bench.dist_setup(None)
     assert (world, rank, pg) == (1, 0, None)
     assert bench.reduce_max(pg, 7.0) == 7.0 and bench.reduce_sum(pg, 7.0) == 7.0
+
+
+def _split_main(rank: int, world: int, port: int, out_dir: str) -> None:
+    # one list of read sets split over the ranks by estimated work; each rank
+    # aligns its share (the oracle stands in for the GPU), rank 0 gathers
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    for sub in ("", "minipoa-rs_b200", "oracle"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import torch.distributed as dist
+
+    import oracle
+    from minipoa_b200 import shard, workloads
+    from minipoa_b200.params import Params
+
+    dist.init_process_group("gloo")
+    sets = workloads.batched_sets(24, seed=77, lmax=500, dmax=10)
+    shares = shard.partition([shard.set_work(s) for s in sets], world)
+    mine = [sets[s] for s in shares[rank]]
+    _, hashes = oracle.batch_run(Params(), mine, kernel=oracle.AUTO_AVX2, threads=1, out_format=2)
+    got = [None] * world
+    dist.all_gather_object(got, hashes)
+    if rank == 0:
+        merged = shard.gather(len(sets), shares, got)
+        with open(os.path.join(out_dir, "split.txt"), "w") as f:
+            f.write(" ".join(str(h) for h in merged) + "\n")
+            f.write(" ".join(str(len(x)) for x in shares) + "\n")
+    dist.destroy_process_group()
+
+
+def test_split_batch_over_two_ranks_equals_single_process(tmp_path):
+    port = _free_port()
+    tmp.start_processes(_split_main, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    merged, sizes = open(tmp_path / "split.txt").read().splitlines()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from minipoa_b200 import workloads
+    from minipoa_b200.params import Params
+
+    sets = workloads.batched_sets(24, seed=77, lmax=500, dmax=10)
+    _, whole = oracle.batch_run(Params(), sets, kernel=oracle.AUTO_AVX2, threads=1, out_format=2)
+    assert [int(x) for x in merged.split()] == whole
+    assert all(int(n) > 0 for n in sizes.split())
+
+
+def test_partition_balances_work_and_covers_every_set():
+    sys.path.insert(0, os.path.join(ROOT, "minipoa-rs_b200"))
+    from minipoa_b200 import shard
+
+    works = [float(w) for w in (100, 90, 80, 70, 60, 50, 40, 30, 20, 10, 5, 5)]
+    for n in (1, 2, 3, 4, 8):
+        sh = shard.partition(works, n)
+        assert sorted(s for x in sh for s in x) == list(range(len(works)))
+        loads = [sum(works[s] for s in x) for x in sh]
+        # LPT: no rank exceeds the best possible by more than the largest set
+        assert max(loads) <= sum(works) / n + max(works)
+    assert shard.partition(works, 3) == shard.partition(works, 3)

@@ -82,3 +82,17 @@ def test_noalloc_rejects_requests_beyond_its_scratch(env):
     # the graph stays usable afterwards
     q = b"ACGTACGAACGT" * 20
     assert _noalloc(mp, _lib, ctx, torch, params, g, q) == _tup(mp.align(params, g, q))
+
+
+def test_noalloc_rejects_a_graph_of_another_context(env):
+    # a graph lives on its own context's stream; aligning it through another
+    # context would read its descriptor before the launch finished
+    mp, _lib, ctx, torch = env
+    params = mp.Params()
+    other = mp.Context(0)
+    g = mp.align_sequences(params, [b"ACGTACGT", b"ACGAACGT"], ctx=other)
+    with pytest.raises(mp.PoaError, match="another context") as e:
+        _noalloc(mp, _lib, ctx, torch, params, g, b"ACGTACGT")
+    assert e.value.code == _lib.POA_ERR_INVALID
+    del g
+    other.close()
