@@ -289,6 +289,27 @@ int poa_probe_int_peak(int32_t device, double *out_ops_per_s);
 int poa_graph_read_gfa(poa_ctx *ctx, const poa_params *params, const char *text, int64_t len, poa_graph **out,
                        char **records, int64_t *records_len);
 
+/* Autotuner (no reference counterpart). Launch settings of the batched
+ * kernel: resident warps per SM and the giant threshold (a set whose
+ * estimated work exceeds giant_factor per-warp shares gets three helper
+ * warps; 0 = none). poa_batch_autotune runs the batch under each candidate
+ * setting, keeps the fastest, applies it and appends it to the cache file
+ * (MINIPOA_B200_TUNE_CACHE, default ~/.cache/minipoa_b200/tune.tsv) under the
+ * batch's size bucket (device, log2 of set count, longest read and mean
+ * depth); poa_batch_create applies a cached setting for its bucket. Results
+ * are the same under every setting. poa_batch_tuning_get reports the current
+ * setting (trials = runs replayed from the captured CUDA graph so far). */
+typedef struct poa_batch_tuning {
+  int32_t warps_per_sm;
+  int32_t reserved;
+  double giant_factor;
+  double device_ms;  /* device time of the chosen setting's run */
+  int32_t trials;
+  int32_t reserved2;
+} poa_batch_tuning;
+int poa_batch_autotune(poa_ctx *ctx, poa_batch *batch, poa_batch_tuning *out);
+int poa_batch_tuning_get(poa_ctx *ctx, poa_batch *batch, poa_batch_tuning *out);
+
 /* Tuning: concurrent warp slots per SM for the batched kernel (0 = auto) and
  * the DP arena bytes per slot (0 = auto from the budget). */
 int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot);

@@ -11,6 +11,8 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <sys/stat.h>
+#include <fstream>
 #include <stdexcept>
 #include <mutex>
 #include <numeric>
@@ -868,8 +870,17 @@ struct poa_batch {
   cudaEvent_t e0 = nullptr, e1 = nullptr, k0 = nullptr, k1 = nullptr;
   bool ran = false;
   uint64_t h2d_bytes = 0, d2h_bytes = 0;
+  std::vector<double> est;     // estimated work per set (size order, giants, tuning bucket)
+  double giant_factor = 1.5;   // giant: estimated work above this many per-warp shares
+  std::string tune_key;        // autotuner cache key of the batch's size bucket
+  // the first pass of a batched run (reset, queue set-up, persistent kernel)
+  // captured once as a CUDA graph and replayed while its launch shape holds
+  cudaGraphExec_t gexec = nullptr;
+  int64_t g_slots = -1, g_slot_bytes = -1;
+  int graph_launches = 0;
 
   ~poa_batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
     if (!ctx) return;
     ctx->dfree(d_read_off, reads_bytes);  // base of the reads allocation
     ctx->dfree(d_matrix, 0);
@@ -883,6 +894,20 @@ struct poa_batch {
     if (e1) cudaEventDestroy(e1);
     if (k0) cudaEventDestroy(k0);
     if (k1) cudaEventDestroy(k1);
+  }
+
+  // Giant jobs: well above the per-warp share of the whole batch, at most
+  // one per SM (the largest ones, which start first, one per SM); none when
+  // giant_factor is 0.
+  void mark_giants() {
+    const double share = std::accumulate(est.begin(), est.end(), 0.0) /
+                         double(std::max(1, ctx->sm_count * batch_resident_warps_per_sm()));
+    for (auto &J : jobs) J.giant = 0;
+    if (giant_factor <= 0) return;
+    for (int64_t k = 0; k < std::min<int64_t>(n_sets, ctx->sm_count); ++k) {
+      const int32_t s = order[size_t(k)];
+      jobs[size_t(s)].giant = est[size_t(s)] > giant_factor * share ? 1 : 0;
+    }
   }
 
   void download_jobs() {
@@ -1339,9 +1364,70 @@ int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *r
 
 // ---- batch
 
-// a job is giant when its estimated work is this many times the average
-// share of one resident warp
-constexpr double GIANT_FACTOR = 1.5;
+// ---- batch autotuner cache
+
+// Tuned launch settings per device and batch size bucket: one line
+// "key<TAB>warps_per_sm<TAB>giant_factor" per bucket in the file named by
+// MINIPOA_B200_TUNE_CACHE (default ~/.cache/minipoa_b200/tune.tsv).
+std::string tune_path() {
+  if (const char *p = std::getenv("MINIPOA_B200_TUNE_CACHE")) return p;
+  const char *home = std::getenv("HOME");
+  return std::string(home ? home : ".") + "/.cache/minipoa_b200/tune.tsv";
+}
+
+int log2_bucket(double x) {
+  int b = 0;
+  while (x >= 2.0 && b < 62) {
+    x /= 2.0;
+    ++b;
+  }
+  return b;
+}
+
+// Size bucket of a batch: device name, log2 of the set count, of the
+// longest read and of the mean depth.
+std::string tune_key(poa_ctx *ctx, int64_t n_sets, const int64_t *set_off, const int64_t *lens) {
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, ctx->device);
+  int64_t mx = 0;
+  for (int64_t r = 0; r < set_off[n_sets]; ++r) mx = std::max(mx, lens[r]);
+  const double depth = n_sets ? double(set_off[n_sets]) / double(n_sets) : 0.0;
+  return std::string(prop.name) + "|sets" + std::to_string(log2_bucket(double(n_sets))) + "|len" +
+         std::to_string(log2_bucket(double(mx))) + "|depth" + std::to_string(log2_bucket(depth));
+}
+
+std::mutex g_tune_mu;
+
+bool tune_lookup(const std::string &key, int *warps_per_sm, double *giant_factor) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  std::ifstream f(tune_path());
+  std::string line;
+  bool found = false;
+  while (std::getline(f, line)) {
+    const size_t a = line.find('\t'), b = a == std::string::npos ? a : line.find('\t', a + 1);
+    if (b == std::string::npos || line.substr(0, a) != key) continue;
+    *warps_per_sm = std::atoi(line.substr(a + 1, b - a - 1).c_str());
+    *giant_factor = std::atof(line.substr(b + 1).c_str());
+    found = true;  // the last entry for a key wins
+  }
+  return found;
+}
+
+void tune_store(const std::string &key, int warps_per_sm, double giant_factor) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  const std::string path = tune_path();
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {
+    std::string dir = path.substr(0, slash), cur;
+    for (size_t i = 0; i <= dir.size(); ++i)
+      if (i == dir.size() || dir[i] == '/') {
+        cur = dir.substr(0, i);
+        if (!cur.empty()) mkdir(cur.c_str(), 0755);
+      }
+  }
+  std::ofstream f(path, std::ios::app);
+  f << key << '\t' << warps_per_sm << '\t' << giant_factor << '\n';
+}
 
 int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, const int64_t *set_off,
                      const uint8_t *const *seqs, const int64_t *lens, poa_batch **out) {
@@ -1440,14 +1526,10 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     b->order.resize(size_t(n_sets));
     std::iota(b->order.begin(), b->order.end(), 0);
     std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return est[a] > est[c]; });
-    // giant jobs: well above the per-warp share of the whole batch, at most
-    // one per SM (the largest ones, which start first, one per SM)
-    const double share = std::accumulate(est.begin(), est.end(), 0.0) /
-                         double(std::max(1, ctx->sm_count * batch_resident_warps_per_sm()));
-    for (int64_t k = 0; k < std::min<int64_t>(n_sets, ctx->sm_count); ++k) {
-      const int32_t s = b->order[size_t(k)];
-      b->jobs[size_t(s)].giant = est[size_t(s)] > GIANT_FACTOR * share ? 1 : 0;
-    }
+    b->est = est;
+    b->tune_key = tune_key(ctx, n_sets, set_off, lens);
+    tune_lookup(b->tune_key, &b->warps_per_sm, &b->giant_factor);
+    b->mark_giants();
     b->upload_jobs();
     b->d_order = (int32_t *)ctx->dalloc(b->order.size() * 4 + 4);
     b->d_queue = (int32_t *)ctx->dalloc(sched_words(b->jobs.size()) * 4);
@@ -1457,6 +1539,58 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     CK(cudaEventCreate(&b->k1));
     CK(cudaStreamSynchronize(ctx->stream));
     *out = b.release();
+  });
+}
+
+int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
+  return api(ctx, [&] {
+    // candidate launch settings: resident warps per SM and the giant
+    // threshold (0: no giant gets helper warps)
+    const int wps_c[] = {8, 8, 8, 6, 4};
+    const double gf_c[] = {1.5, 3.0, 0.0, 1.5, 1.5};
+    const int keep_w = b->warps_per_sm;
+    const double keep_g = b->giant_factor;
+    double best_ms = 0;
+    int best_w = keep_w;
+    double best_g = keep_g;
+    int tried = 0;
+    for (int k = 0; k < 5; ++k) {
+      b->warps_per_sm = wps_c[k];
+      b->giant_factor = gf_c[k];
+      b->mark_giants();
+      b->upload_jobs();
+      poa_batch_stats st{};
+      const int rc = poa_batch_run(ctx, b, 0, &st);
+      if (rc != POA_OK) throw AlignError{rc, t_last_error};
+      ++tried;
+      if (tried == 1 || st.device_ms < best_ms) {
+        best_ms = st.device_ms;
+        best_w = wps_c[k];
+        best_g = gf_c[k];
+      }
+    }
+    b->warps_per_sm = best_w;
+    b->giant_factor = best_g;
+    b->mark_giants();
+    b->upload_jobs();
+    tune_store(b->tune_key, best_w, best_g);
+    if (out) {
+      out->warps_per_sm = best_w;
+      out->reserved = 0;
+      out->giant_factor = best_g;
+      out->device_ms = best_ms;
+      out->trials = tried;
+    }
+  });
+}
+
+int poa_batch_tuning_get(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
+  return api(ctx, [&] {
+    out->warps_per_sm = b->warps_per_sm > 0 ? b->warps_per_sm : batch_resident_warps_per_sm();
+    out->reserved = 0;
+    out->giant_factor = b->giant_factor;
+    out->device_ms = 0;
+    out->trials = b->graph_launches;
   });
 }
 
@@ -1483,8 +1617,10 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
     int passes = 0, launches = 0;
     double kernel_ms = 0;
     CK(cudaEventRecord(b->e0, ctx->stream));
-    CK(launch_reset(b->d_jobs, int(b->n_sets), b->sigma, b->unknown, ctx->stream));
-    ++launches;
+    if (mode != 0) {
+      CK(launch_reset(b->d_jobs, int(b->n_sets), b->sigma, b->unknown, ctx->stream));
+      ++launches;
+    }
     int slots_first = 0;
     if (mode == 0) {
       std::vector<int32_t> pending = b->order;
@@ -1494,15 +1630,47 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
         int64_t slot_bytes = b->arena_pool / slots / 256 * 256;
         if (b->slot_bytes_override && passes == 0)
           slot_bytes = std::min<int64_t>(int64_t(b->slot_bytes_override), slot_bytes);
-        if (passes == 0) slots_first = int(slots);
-        CK(cudaMemcpyAsync(b->d_order, pending.data(), pending.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemsetAsync(b->d_queue, 0, sched_words(pending.size()) * 4, ctx->stream));
-        CK(cudaEventRecord(b->k0, ctx->stream));
-        CK(launch_batch(b->d_jobs, b->d_order, int(pending.size()), b->d_queue, ctx->sm_count, b->P, b->arenas,
-                        slot_bytes,
-                        int(slots), ctx->stream));
-        CK(cudaEventRecord(b->k1, ctx->stream));
-        ++launches;
+        if (passes == 0) {
+          slots_first = int(slots);
+          // the first pass as one CUDA graph (reset of every graph, queue
+          // set-up, the persistent kernel), captured once per launch shape
+          if (!b->gexec || b->g_slots != slots || b->g_slot_bytes != slot_bytes) {
+            if (b->gexec) cudaGraphExecDestroy(b->gexec);
+            b->gexec = nullptr;
+            CK(prepare_batch_kernel());
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t ce = launch_reset(b->d_jobs, int(b->n_sets), b->sigma, b->unknown, ctx->stream);
+            if (ce == cudaSuccess)
+              ce = cudaMemcpyAsync(b->d_order, b->order.data(), b->order.size() * 4, cudaMemcpyHostToDevice,
+                                   ctx->stream);
+            if (ce == cudaSuccess)
+              ce = cudaMemsetAsync(b->d_queue, 0, sched_words(b->order.size()) * 4, ctx->stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(b->k0, ctx->stream);
+            if (ce == cudaSuccess)
+              ce = launch_batch(b->d_jobs, b->d_order, int(b->order.size()), b->d_queue, ctx->sm_count, b->P,
+                                b->arenas, slot_bytes, int(slots), ctx->stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(b->k1, ctx->stream);
+            const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
+            if (ce == cudaSuccess) ce = ee;
+            if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->gexec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            CK(ce);
+            b->g_slots = slots;
+            b->g_slot_bytes = slot_bytes;
+          }
+          CK(cudaGraphLaunch(b->gexec, ctx->stream));
+          ++b->graph_launches;
+          launches += 2;
+        } else {
+          CK(cudaMemcpyAsync(b->d_order, pending.data(), pending.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+          CK(cudaMemsetAsync(b->d_queue, 0, sched_words(pending.size()) * 4, ctx->stream));
+          CK(cudaEventRecord(b->k0, ctx->stream));
+          CK(launch_batch(b->d_jobs, b->d_order, int(pending.size()), b->d_queue, ctx->sm_count, b->P, b->arenas,
+                          slot_bytes, int(slots), ctx->stream));
+          CK(cudaEventRecord(b->k1, ctx->stream));
+          ++launches;
+        }
         ++passes;
         b->download_jobs();
         float kms = 0;

@@ -14,6 +14,9 @@ namespace poa {
 // one claim flag per queue position.
 constexpr int SCHED_SM_SLOTS = 512, SCHED_LEVELS = 64;
 inline size_t sched_words(size_t n_jobs) { return 4 + SCHED_SM_SLOTS + SCHED_LEVELS + n_jobs; }
+// Sets the batched kernel's launch attributes (once per process); launch_batch
+// calls it, and a caller capturing a launch into a CUDA graph calls it first.
+cudaError_t prepare_batch_kernel();
 cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
                          const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream);
 cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,

@@ -335,13 +335,7 @@ __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   J->order_exact = 1;
 }
 
-cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
-                         const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
-  // fewer slots than a full machine: narrower blocks, so that the warps
-  // spread over all SMs instead of filling a few
-  int wpb = WARPS_PER_BLOCK;
-  if (num_sms > 0 && slots < num_sms * WARPS_PER_BLOCK) wpb = std::max(1, (slots + num_sms - 1) / num_sms);
-  const int blocks = (slots + wpb - 1) / wpb;
+cudaError_t prepare_batch_kernel() {
   static bool attr = false;
   if (!attr) {
     const cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -349,6 +343,18 @@ cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, 
     if (e != cudaSuccess) return e;
     attr = true;
   }
+  return cudaSuccess;
+}
+
+cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, int32_t *sched, int num_sms,
+                         const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream) {
+  // fewer slots than a full machine: narrower blocks, so that the warps
+  // spread over all SMs instead of filling a few
+  int wpb = WARPS_PER_BLOCK;
+  if (num_sms > 0 && slots < num_sms * WARPS_PER_BLOCK) wpb = std::max(1, (slots + num_sms - 1) / num_sms);
+  const int blocks = (slots + wpb - 1) / wpb;
+  const cudaError_t pe = prepare_batch_kernel();
+  if (pe != cudaSuccess) return pe;
   k_batch<<<blocks, wpb * 32, wpb * sizeof(WarpSmem), stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, sched,
                                                                 num_sms, P, arenas, slot_bytes, slots);
   return cudaGetLastError();

@@ -58,6 +58,11 @@ class BatchStats(ctypes.Structure):
                 ("phase_cycles", ctypes.c_uint64 * 4)]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("warps_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32), ("giant_factor", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("trials", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
+
+
 # name -> (restype, argtypes); every function declared in include/minipoa_b200.h
 P = ctypes.POINTER
 _vp = ctypes.c_void_p
@@ -101,6 +106,8 @@ SIGNATURES = {
     "poa_batch_graph": (ctypes.c_int, [_vp, _vp, _i64, P(_vp)]),
     "poa_batch_free": (None, [_vp]),
     "poa_batch_tune": (ctypes.c_int, [_vp, _vp, _i32, _u64]),
+    "poa_batch_autotune": (ctypes.c_int, [_vp, _vp, P(BatchTuning)]),
+    "poa_batch_tuning_get": (ctypes.c_int, [_vp, _vp, P(BatchTuning)]),
     "poa_probe_int_peak": (ctypes.c_int, [_i32, P(ctypes.c_double)]),
     "poa_align_noalloc": (ctypes.c_int, [_vp, _cp, _vp, _vp, _i64, _vp, _i64, _vp]),
     "poa_batch_transfer_bytes": (ctypes.c_int, [_vp, _vp, P(_u64), P(_u64)]),

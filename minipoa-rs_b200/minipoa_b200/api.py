@@ -357,6 +357,18 @@ class Batch:
         except Exception:
             pass
 
+    def autotune(self) -> _lib.BatchTuning:
+        """Runs the batch under each candidate launch setting, applies and
+        caches the fastest (results are identical under every setting)."""
+        t = _lib.BatchTuning()
+        self.ctx.check(self.L.poa_batch_autotune(self.ctx.h, self.h, ctypes.byref(t)))
+        return t
+
+    def tuning(self) -> _lib.BatchTuning:
+        t = _lib.BatchTuning()
+        self.ctx.check(self.L.poa_batch_tuning_get(self.ctx.h, self.h, ctypes.byref(t)))
+        return t
+
     def tune(self, warps_per_sm: int = 0, arena_bytes_per_slot: int = 0):
         self.ctx.check(self.L.poa_batch_tune(self.ctx.h, self.h, warps_per_sm, arena_bytes_per_slot))
 
