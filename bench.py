@@ -61,7 +61,7 @@ def parse():
                          "--sets sets per rank (weak scaling)")
     ap.add_argument("--serve-jobs", type=int, default=1024, help="jobs of the serving loop's saturation run (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="length of the serving run at 80%% load")
-    ap.add_argument("--seeded-reads", type=int, default=20,
+    ap.add_argument("--seeded-reads", type=int, default=100,
                     help="reads of the seeded-window run (16.5 kbp ancestor, ~5%% error; 0: skip)")
     return ap.parse_args()
 
@@ -244,22 +244,52 @@ def consensus_parity(gpu_text: bytes, hashes: dict):
             "mismatched_sets": bad[:16]}
 
 
-def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006):
-    """Serving loop (continuous batching) on jobs drawn from the batched
-    workload's distribution: saturated throughput (all jobs submitted at
-    once), then Poisson arrivals at 80% of it, with each job's latency from
-    submission to completion (measured by the server)."""
-    import random
+def serving_jobs(mp, params, ctx, n_jobs: int, seed: int = 1006):
+    """Jobs drawn like the batched workload (ancestor 200-5000 bp log-uniform,
+    error 2-15% split 60/20/20); 20% of them bring an initial graph: the GFA
+    of 10-40 prior reads (aligned here in one batched launch and written with
+    Graph::gfa) plus 5-20 new reads to extend it; the others are plain read
+    sets of depth 10-60."""
+    import numpy as np
 
     from minipoa_b200 import workloads
 
-    jobs = workloads.batched_sets(n_jobs, seed=seed)
-    server = mp.Server(params, ctx=ctx)
+    rng = np.random.default_rng(seed)
+    jobs, prior_sets, gfa_jobs = [], [], []
+    for k in range(n_jobs):
+        L = int(np.exp(rng.uniform(np.log(200), np.log(5000))))
+        e = float(rng.uniform(0.02, 0.15))
+        if rng.random() < 0.2:
+            k0, k1 = int(rng.integers(10, 41)), int(rng.integers(5, 21))
+            reads = workloads.read_set(rng, L, k0 + k1, 0.6 * e, 0.2 * e, 0.2 * e)
+            prior_sets.append(reads[:k0])
+            gfa_jobs.append(k)
+            jobs.append([None, reads[k0:]])
+        else:
+            jobs.append([None, workloads.read_set(rng, L, int(rng.integers(10, 61)), 0.6 * e, 0.2 * e, 0.2 * e)])
+    if prior_sets:
+        pb = mp.Batch(params, prior_sets, ctx)
+        pb.run(0)
+        for k, s in zip(gfa_jobs, range(len(prior_sets))):
+            jobs[k][0] = pb.output(s, 2)
+        del pb
+    return jobs
+
+
+def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006, pool_gb: float = 120.0):
+    """Serving loop (continuous batching) on serving_jobs: saturated
+    throughput (all jobs submitted at once), then Poisson arrivals at 80% of
+    it, with each job's latency from submission to completion (measured by
+    the server), split into queueing and running time, per job-size bucket."""
+    import random
+
+    jobs = serving_jobs(mp, params, ctx, n_jobs, seed)
+    server = mp.Server(params, ctx=ctx, pool_bytes=int(pool_gb * 1e9) // 256 * 256)
     t0 = time.perf_counter()
-    ids = [server.submit(j) for j in jobs]
+    ids = [server.submit(r, gfa=g) for g, r in jobs]
     cells = 0
     for i in ids:
-        server.wait(i, 120000.0)
+        server.wait(i, 300000.0)
         cells += server.info(i).cells
     sat_s = time.perf_counter() - t0
     print(f"[bench] serving: {n_jobs} jobs at once in {sat_s:.2f} s", file=sys.stderr, flush=True)
@@ -268,7 +298,7 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
     sat_rate = n_jobs / sat_s
     rate = 0.8 * sat_rate
     rng = random.Random(seed)
-    submitted, lat, load_cells = [], [], [0]
+    submitted, recs = [], []
     done = threading.Event()
 
     def reaper():
@@ -277,11 +307,10 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
             if k >= len(submitted):
                 time.sleep(0.0005)
                 continue
-            j = submitted[k]
-            server.wait(j, 120000.0)
+            j, kind = submitted[k]
+            server.wait(j, 300000.0)
             info = server.info(j)
-            lat.append(info.latency_ms)
-            load_cells[0] += info.cells
+            recs.append((info.latency_ms, info.queued_ms, info.cells, kind))
             server.release(j)
             k += 1
 
@@ -294,7 +323,8 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
         if now < t_next:
             time.sleep(min(t_next - now, 0.002))
             continue
-        submitted.append(server.submit(jobs[rng.randrange(n_jobs)]))
+        g, r = jobs[rng.randrange(n_jobs)]
+        submitted.append((server.submit(r, gfa=g), "gfa" if g is not None else "plain"))
         t_next += rng.expovariate(rate)
     done.set()
     th.join()
@@ -302,40 +332,119 @@ def serving_bench(mp, params, ctx, n_jobs: int, seconds: float, seed: int = 1006
     print(f"[bench] serving: {len(submitted)} Poisson arrivals at {rate:.0f}/s, drained in {span:.2f} s",
           file=sys.stderr, flush=True)
     server.close()
-    lat.sort()
-    pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None  # noqa: E731
-    return {"workload": f"{n_jobs} jobs drawn like the batched workload (seed {seed})",
+
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(q * len(v)))] if v else None
+
+    def summary(rows):
+        return {"jobs": len(rows), "p50_ms": pct([r[0] for r in rows], 0.50), "p99_ms": pct([r[0] for r in rows], 0.99),
+                "queued_p50_ms": pct([r[1] for r in rows], 0.50), "queued_p99_ms": pct([r[1] for r in rows], 0.99),
+                "run_p50_ms": pct([r[0] - r[1] for r in rows], 0.50),
+                "run_p99_ms": pct([r[0] - r[1] for r in rows], 0.99)}
+
+    buckets = {"small (<10 M cells)": [r for r in recs if r[2] < 10e6],
+               "medium (10-100 M cells)": [r for r in recs if 10e6 <= r[2] < 100e6],
+               "large (>=100 M cells)": [r for r in recs if r[2] >= 100e6]}
+    lat = [r[0] for r in recs]
+    return {"workload": f"{n_jobs} jobs drawn like the batched workload, 20% extending a GFA graph of 10-40 prior "
+                        f"reads with 5-20 new reads (seed {seed}); pool {pool_gb:g} GB",
             "saturated_jobs_per_s": sat_rate, "saturated_gcups": cells / sat_s / 1e9,
             "load": "Poisson arrivals at 80% of the saturated job rate", "arrival_jobs_per_s": rate,
-            "jobs": len(lat), "gcups": load_cells[0] / span / 1e9,
-            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None}
+            "jobs": len(recs), "gcups": sum(r[2] for r in recs) / span / 1e9,
+            "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "max_ms": max(lat) if lat else None,
+            "all": summary(recs), "by_size": {k: summary(v) for k, v in buckets.items()},
+            "gfa_jobs": summary([r for r in recs if r[3] == "gfa"])}
 
 
-def seeded_bench(mp, ctx, n_reads: int, seed: int = 1002):
-    """Seeded windowed POA (-S -B -r1) on a 16.5 kbp ancestor with reads at
+def cpu_seeded(mp, params, reads, threads: int):
+    """The seeded read loop on the CPU (the CPU baseline of the seeded
+    workload): per read, the oracle graph's consensus, the seed windows from
+    the same host function the GPU path uses (a shared input: the reference's
+    own minimizer crate is not available), each window aligned with the
+    oracle's poa on a pool of `threads` host threads (the reference's
+    map_ordered over windows, src/align.rs:186) and the anchor nodes added as
+    align::align does; then add_path and toposort. Returns (graph, windows)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle
+
+    og = oracle.OracleGraph(params)
+    n_win = 0
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for r, q in enumerate(reads):
+            if og.n_nodes() <= 2:
+                items = [(0, params.encode("N"), None)] + [(None, params.encode(c), None) for c in q]
+            else:
+                cons, ids, _ = og.consensus(params)
+                anchors, tail = mp.anchor_windows(params, q, cons)
+                windows, beg, qbeg, prev, ok = [], 0, 0, None, bool(anchors)
+                for a in anchors:
+                    ts, qs = a.target_end + 1 - a.span, a.query_end + 1 - a.span
+                    if not (a.span > 0 and a.target_end < len(ids) and a.query_end < len(q) and qs >= qbeg
+                            and (prev is None or ts > prev)
+                            and all(params.encode(cons[ts + o]) == params.encode(q[qs + o]) for o in range(a.span))):
+                        ok = False
+                        break
+                    windows.append((beg, ids[ts], qbeg, qs, a.adaptive_before, ids[ts:a.target_end]))
+                    beg, qbeg, prev = ids[a.target_end], a.query_end + 1, a.target_end
+                if ok:
+                    windows.append((beg, 1, qbeg, len(q), tail, []))
+                    base = og.dump(len(params.alphabet))["base"]
+                    parts = list(ex.map(lambda w: og.poa(params, w[0], w[1], q[w[2]:w[3]], w[4],
+                                                         params.b if w[4] else params.win_band,
+                                                         kernel=oracle.AUTO_AVX2), windows))
+                    items = []
+                    for w, part in zip(windows, parts):
+                        items += part + [(i, base[i], None) for i in w[5]]
+                    n_win += len(windows)
+                else:
+                    items = og.poa(params, 0, 1, q, True, params.b, kernel=oracle.AUTO_AVX2)
+            og.add_path(params, r, items)
+            og.toposort()
+    return og, n_win
+
+
+def seeded_bench(mp, ctx, n_reads: int, plain_reads: int = 20, seed: int = 1002, threads: int = 0):
+    """Seeded windowed POA (-S -B -r1) on a 16.5 kbp ancestor with 100 reads at
     about 5% error (3/1/1% sub/ins/del, indel lengths geometric with mean
     1.5): windows/s with all windows of a read in one launch (one warp per
-    window) and with one launch per window, on the same reads."""
+    window) on every read; the same with one launch per window on the first
+    `plain_reads` reads (the batched/plain ratio is taken on those); and the
+    CPU loop (cpu_seeded) on all host threads, with MSA bytes compared."""
     from minipoa_b200 import workloads
     from minipoa_b200.params import Params
 
+    threads = threads or os.cpu_count() or 1
     reads = workloads.seeded_window_set(seed)[:n_reads]
     params = Params(seeding=True, adaptive=True, result=1)
-    out = {"workload": f"16,500 bp ancestor, first {len(reads)} of 100 reads (seed {seed}), -S -B -r1"}
-    msa = {}
-    for name, plain in (("batched", False), ("plain", True)):
+    recs = [mp.Sequence(name=f"read{i}", seq=r) for i, r in enumerate(reads)]
+    out = {"workload": f"16,500 bp ancestor, {len(reads)} reads (seed {seed}), -S -B -r1"}
+
+    def gpu(rs, plain):
         ctx.tune_windows(plain)
         w0 = ctx.window_stats()
         t0 = time.perf_counter()
-        g = mp.align_sequences(params, reads, ctx=ctx)
+        g = mp.align_sequences(params, rs, ctx=ctx)
         dt = time.perf_counter() - t0
         w1 = ctx.window_stats()
-        msa[name] = g.msa(params, [mp.Sequence(name=f"read{i}", seq=r) for i, r in enumerate(reads)])
-        out[name] = {"windows": w1[0] - w0[0], "launches": w1[1] - w0[1], "fallback_reads": w1[2] - w0[2],
-                     "seconds": dt, "windows_per_s": (w1[0] - w0[0]) / dt, "reads_per_s": len(reads) / dt}
-    ctx.tune_windows(False)
-    out["identical_msa"] = msa["batched"] == msa["plain"]
-    out["batched_over_plain"] = out["batched"]["windows_per_s"] / out["plain"]["windows_per_s"]
+        ctx.tune_windows(False)
+        return g, {"reads": len(rs), "windows": w1[0] - w0[0], "launches": w1[1] - w0[1],
+                   "fallback_reads": w1[2] - w0[2], "seconds": dt, "windows_per_s": (w1[0] - w0[0]) / dt,
+                   "reads_per_s": len(rs) / dt}
+
+    g_all, out["batched"] = gpu(reads, False)
+    gp_b, out["batched_first"] = gpu(reads[:plain_reads], False)
+    gp_p, out["plain_first"] = gpu(reads[:plain_reads], True)
+    sub = recs[:plain_reads]
+    out["identical_msa_batched_plain"] = gp_b.msa(params, sub) == gp_p.msa(params, sub)
+    out["batched_over_plain"] = out["batched_first"]["windows_per_s"] / out["plain_first"]["windows_per_s"]
+    t0 = time.perf_counter()
+    og, n_win = cpu_seeded(mp, params, reads, threads)
+    dt = time.perf_counter() - t0
+    out["cpu"] = {"threads": threads, "seconds": dt, "windows": n_win, "windows_per_s": n_win / dt,
+                  "kind": "oracle poa per window on a thread pool, windows from the same host seeding"}
+    out["identical_msa_gpu_cpu"] = g_all.msa(params, recs) == og.msa(params, recs)
     return out
 
 

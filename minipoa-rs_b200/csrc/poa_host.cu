@@ -1951,6 +1951,7 @@ struct ServerJob {
   std::unique_ptr<BuildGraph> init;
   std::vector<int32_t> init_rank, init_order;
   int32_t existing = 0;
+  int skips = 0;  // admission rounds that passed this job over at the head of the queue
   Caps caps;
   uint64_t storage_bytes = 0, reads_bytes = 0, arena_bytes = 0;
   char *storage = nullptr, *reads = nullptr, *arena = nullptr;
@@ -1988,6 +1989,10 @@ struct poa_server {
   std::vector<Wave> waves;
   std::vector<cudaStream_t> streams;
   std::vector<int> free_streams;
+  // pinned staging of the reads a wave uploads, one buffer per stream slot
+  // (reused once the slot's wave has finished, so no copy waits on the host)
+  std::vector<char *> stage;
+  std::vector<size_t> stage_bytes;
   cudaStream_t out_stream = nullptr;
   std::thread worker;
   bool stop = false;
@@ -2014,6 +2019,8 @@ struct poa_server {
       cudaEventDestroy(w.done);
     }
     for (auto st : streams) cudaStreamDestroy(st);
+    for (char *p : stage)
+      if (p) cudaFreeHost(p);
     if (out_stream) cudaStreamDestroy(out_stream);
     if (h_done) cudaFreeHost(h_done);
     if (ctx) ctx->dfree(pool_mem, pool_bytes);
@@ -2142,8 +2149,14 @@ bool poa_server::launch_wave() {
   {
     std::lock_guard<std::mutex> lk(mu);
     if (pending.empty() || free_streams.empty()) return false;
-    while (!pending.empty() && adm.size() < free_done.size()) {
-      ServerJob &sj = *jobs.at(pending.front());
+    // Admission in arrival order, looking past a job that does not fit into
+    // the free pool for up to kLookahead later jobs that do; a head job
+    // passed over kMaxSkips times holds back the jobs behind it, so a large
+    // job is not starved by a stream of small ones.
+    constexpr int kLookahead = 32, kMaxSkips = 8;
+    int passed = 0;
+    for (size_t pi = 0; pi < pending.size() && adm.size() < free_done.size();) {
+      ServerJob &sj = *jobs.at(pending[pi]);
       char *st = sj.storage ? sj.storage : pool.take(sj.storage_bytes);
       char *rd = sj.reads ? sj.reads : (st ? pool.take(sj.reads_bytes) : nullptr);
       char *ar = (st && rd) ? pool.take(sj.arena_bytes) : nullptr;
@@ -2157,16 +2170,19 @@ bool poa_server::launch_wave() {
           sj.state = POA_SERVER_FAILED;
           sj.error = "job needs more device memory than the server pool";
           sj.t_done = now_s();
-          pending.pop_front();
+          pending.erase(pending.begin() + long(pi));
           cv.notify_all();
           continue;
         }
-        break;
+        if (pi == 0 && ++sj.skips > kMaxSkips) break;
+        if (++passed > kLookahead) break;
+        ++pi;
+        continue;
       }
       sj.storage = st;
       sj.reads = rd;
       sj.arena = ar;
-      pending.pop_front();
+      pending.erase(pending.begin() + long(pi));
       adm.push_back(&sj);
     }
     if (adm.empty()) return false;
@@ -2192,6 +2208,18 @@ bool poa_server::launch_wave() {
   const double t = now_s();
   std::vector<Job> hj(adm.size());
   int n_fresh = 0;
+  size_t need = adm.size() * (sizeof(Job) + 4) + 256;  // descriptors and queue
+  for (ServerJob *j : adm)
+    if (j->fresh) need += (j->reads_bytes + 255) / 256 * 256;
+  if (stage_bytes[size_t(w.stream)] < need) {
+    if (stage[size_t(w.stream)]) cudaFreeHost(stage[size_t(w.stream)]);
+    stage[size_t(w.stream)] = nullptr;
+    stage_bytes[size_t(w.stream)] = 0;
+    CK(cudaHostAlloc(reinterpret_cast<void **>(&stage[size_t(w.stream)]), need, cudaHostAllocDefault));
+    stage_bytes[size_t(w.stream)] = need;
+  }
+  char *staging = stage[size_t(w.stream)];
+  size_t staged = 0;
   for (size_t k = 0; k < adm.size(); ++k) {
     ServerJob &sj = *adm[k];
     if (sj.fresh) {
@@ -2211,16 +2239,17 @@ bool poa_server::launch_wave() {
       J.read_len = reinterpret_cast<int32_t *>(sj.reads + n * 8);
       J.reads = reinterpret_cast<uint8_t *>(sj.reads + n * 12);
       J.n_reads = int32_t(n);
-      std::vector<char> host(sj.reads_bytes, 0);
+      char *host = staging + staged;
+      staged += (sj.reads_bytes + 255) / 256 * 256;
+      std::memset(host, 0, sj.reads_bytes);
       int64_t at = 0;
       for (int64_t r = 0; r < n; ++r) {
-        reinterpret_cast<int64_t *>(host.data())[r] = at;
-        reinterpret_cast<int32_t *>(host.data() + n * 8)[r] = int32_t(sj.lens[size_t(r)]);
+        reinterpret_cast<int64_t *>(host)[r] = at;
+        reinterpret_cast<int32_t *>(host + n * 8)[r] = int32_t(sj.lens[size_t(r)]);
         at += sj.lens[size_t(r)];
       }
-      if (!sj.bytes.empty()) std::memcpy(host.data() + n * 12, sj.bytes.data(), sj.bytes.size());
-      CK(cudaMemcpyAsync(sj.reads, host.data(), sj.reads_bytes, cudaMemcpyHostToDevice, stream));
-      CK(cudaStreamSynchronize(stream));  // the staging vector goes out of scope
+      if (!sj.bytes.empty()) std::memcpy(host + n * 12, sj.bytes.data(), sj.bytes.size());
+      CK(cudaMemcpyAsync(sj.reads, host, sj.reads_bytes, cudaMemcpyHostToDevice, stream));
       sj.J = J;
       sj.t_start = t;
     }
@@ -2242,10 +2271,32 @@ bool poa_server::launch_wave() {
   w.d_jobs = reinterpret_cast<Job *>(m);
   int32_t *d_order = reinterpret_cast<int32_t *>(m + PoolAlloc::round(hj.size() * sizeof(Job)));
   int32_t *d_sched = d_order + (hj.size() + 63) / 64 * 64;
+  // the wave's queue: largest estimated work first
   std::vector<int32_t> order(hj.size());
   std::iota(order.begin(), order.end(), 0);
-  CK(cudaMemcpyAsync(w.d_jobs, hj.data(), hj.size() * sizeof(Job), cudaMemcpyHostToDevice, stream));
-  CK(cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, stream));
+  std::vector<double> work(adm.size());
+  for (size_t k = 0; k < adm.size(); ++k) {
+    double sum = 0;
+    for (int64_t l : adm[k]->lens) sum += double(l);
+    work[k] = sum * double(first_arena(*adm[k]));
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return work[size_t(a)] > work[size_t(c)]; });
+  // descriptors and queue through the wave's pinned staging (after the reads)
+  const size_t jb = hj.size() * sizeof(Job), ob = order.size() * 4;
+  if (staged + jb + ob > stage_bytes[size_t(w.stream)]) {
+    CK(cudaStreamSynchronize(stream));  // the reads already staged are in flight
+    if (stage[size_t(w.stream)]) cudaFreeHost(stage[size_t(w.stream)]);
+    stage[size_t(w.stream)] = nullptr;
+    stage_bytes[size_t(w.stream)] = 0;
+    CK(cudaHostAlloc(reinterpret_cast<void **>(&stage[size_t(w.stream)]), jb + ob + 256, cudaHostAllocDefault));
+    stage_bytes[size_t(w.stream)] = jb + ob + 256;
+    staging = stage[size_t(w.stream)];
+    staged = 0;
+  }
+  std::memcpy(staging + staged, hj.data(), jb);
+  std::memcpy(staging + staged + jb, order.data(), ob);
+  CK(cudaMemcpyAsync(w.d_jobs, staging + staged, jb, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_order, staging + staged + jb, ob, cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d_sched, 0, sched_words(hj.size()) * 4, stream));
   if (n_fresh) CK(launch_reset(w.d_jobs, n_fresh, P.sigma, P.unknown, stream));
   CK(launch_batch(w.d_jobs, d_order, int(hj.size()), d_sched, ctx->sm_count, P, nullptr, 0, int(hj.size()), stream));
@@ -2334,6 +2385,8 @@ int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_byte
       sv->streams.push_back(st);
       sv->free_streams.push_back(k);
     }
+    sv->stage.assign(size_t(streams), nullptr);
+    sv->stage_bytes.assign(size_t(streams), 0);
     CK(cudaStreamCreateWithFlags(&sv->out_stream, cudaStreamNonBlocking));
     constexpr int kDoneSlots = 1 << 16;
     CK(cudaHostAlloc(reinterpret_cast<void **>(&sv->h_done), kDoneSlots * 4, cudaHostAllocMapped));
