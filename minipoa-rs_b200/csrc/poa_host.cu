@@ -544,6 +544,9 @@ int api(poa_ctx *ctx, F &&f) {
     t_last_error = e.msg;
     return e.code;
   } catch (const CudaError &e) {
+    // a non-sticky error stays the runtime's "last error" until read; clear
+    // it so the next call's launch check does not report it again
+    cudaGetLastError();
     t_last_error = std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")";
     return POA_ERR_CUDA;
   } catch (const std::bad_alloc &) {
@@ -861,7 +864,7 @@ struct poa_batch {
   std::vector<Caps> caps;
   Job *d_jobs = nullptr;
   std::vector<int32_t> order;
-  int32_t *d_order = nullptr;
+  int32_t *d_order = nullptr;  // the pass's job order, then (at base_order()) the first pass's
   int32_t *d_queue = nullptr;
   char *arenas = nullptr;
   int64_t arena_pool = 0;
@@ -879,6 +882,13 @@ struct poa_batch {
   int64_t g_slots = -1, g_slot_bytes = -1;
   int graph_launches = 0;
 
+  // d_order holds two orders: the running pass's, and at base_order() the
+  // size order of the first pass, uploaded once so the captured first pass
+  // copies it on the device
+  size_t order_half() const { return (order.size() + 4) / 4 * 4; }
+  size_t order_bytes() const { return 2 * order_half() * 4; }
+  int32_t *base_order() const { return d_order + order_half(); }
+
   ~poa_batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (!ctx) return;
@@ -887,7 +897,7 @@ struct poa_batch {
     ctx->dfree(d_encode, 0);
     ctx->dfree(storage, storage_bytes);
     ctx->dfree(d_jobs, jobs.size() * sizeof(Job));
-    ctx->dfree(d_order, order.size() * 4 + 4);
+    ctx->dfree(d_order, order_bytes());
     ctx->dfree(d_queue, sched_words(jobs.size()) * 4);
     ctx->dfree(arenas, size_t(arena_pool));
     if (e0) cudaEventDestroy(e0);
@@ -1531,8 +1541,9 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     tune_lookup(b->tune_key, &b->warps_per_sm, &b->giant_factor);
     b->mark_giants();
     b->upload_jobs();
-    b->d_order = (int32_t *)ctx->dalloc(b->order.size() * 4 + 4);
+    b->d_order = (int32_t *)ctx->dalloc(b->order_bytes());
     b->d_queue = (int32_t *)ctx->dalloc(sched_words(b->jobs.size()) * 4);
+    CK(cudaMemcpyAsync(b->base_order(), b->order.data(), b->order.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaEventCreate(&b->e0));
     CK(cudaEventCreate(&b->e1));
     CK(cudaEventCreate(&b->k0));
@@ -1642,15 +1653,13 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
             CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
             cudaError_t ce = launch_reset(b->d_jobs, int(b->n_sets), b->sigma, b->unknown, ctx->stream);
             if (ce == cudaSuccess)
-              ce = cudaMemcpyAsync(b->d_order, b->order.data(), b->order.size() * 4, cudaMemcpyHostToDevice,
+              ce = cudaMemcpyAsync(b->d_order, b->base_order(), b->order.size() * 4, cudaMemcpyDeviceToDevice,
                                    ctx->stream);
             if (ce == cudaSuccess)
               ce = cudaMemsetAsync(b->d_queue, 0, sched_words(b->order.size()) * 4, ctx->stream);
-            if (ce == cudaSuccess) ce = cudaEventRecord(b->k0, ctx->stream);
             if (ce == cudaSuccess)
               ce = launch_batch(b->d_jobs, b->d_order, int(b->order.size()), b->d_queue, ctx->sm_count, b->P,
                                 b->arenas, slot_bytes, int(slots), ctx->stream);
-            if (ce == cudaSuccess) ce = cudaEventRecord(b->k1, ctx->stream);
             const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
             if (ce == cudaSuccess) ce = ee;
             if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->gexec, graph, 0);
@@ -1659,7 +1668,11 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
             b->g_slots = slots;
             b->g_slot_bytes = slot_bytes;
           }
+          // timing events stay outside the graph: an event recorded during
+          // capture becomes a dependency marker, not a timestamp
+          CK(cudaEventRecord(b->k0, ctx->stream));
           CK(cudaGraphLaunch(b->gexec, ctx->stream));
+          CK(cudaEventRecord(b->k1, ctx->stream));
           ++b->graph_launches;
           launches += 2;
         } else {
@@ -2525,7 +2538,8 @@ int poa_server_output(poa_ctx *ctx, poa_server *sv, int64_t job, int32_t result,
       if (sj.state == POA_SERVER_FAILED) throw AlignError{POA_ERR_ALIGN, sj.error};
       if (sj.state != POA_SERVER_DONE) throw AlignError{POA_ERR_INVALID, "job has not finished"};
       J = sj.J;
-      k = int64_t(sj.lens.size());
+      // sequence ids: the imported graph's path records, then the new reads
+      k = int64_t(sj.existing) + int64_t(sj.lens.size());
       words = uint64_t(packed_words(J, sigma));
       tmp_bytes = 1024 + words * 4 + 16;
       tmp = sv->pool.take(tmp_bytes);
