@@ -240,7 +240,7 @@ typedef struct poa_batch_stats {
   uint64_t rows_g4;     /* DP rows of the 4-stripe tile (385-512 columns) */
   uint64_t rows_generic;  /* DP rows of the generic row (wider, > 32 predecessors, i64) */
   int32_t coop_jobs;    /* jobs that ran cooperative rows (a giant with helper warps) */
-  int32_t reserved2;
+  int32_t wave_reads;   /* reads whose static-band DP ran as a row wavefront (lane per row) */
   uint64_t phase_cycles[4]; /* profiling builds only (POA_PHASE_CYCLES), else 0: warp cycles
                                in band guides, DP rows, traceback, graph update */
 } poa_batch_stats;
@@ -318,42 +318,46 @@ int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_
  * runs one job per process). Continuous batching: jobs (each one
  * extend_graph over its reads, src/lib.rs:184-204, on a new graph) are
  * submitted at any time; a dispatcher thread admits them in arrival order
- * while the server's device pool holds their graph storage, reads and DP
- * arena, and launches each admission round as one wave of the batched kernel
- * on its own stream, so waves overlap on the device. A job's completion is
- * seen as soon as its own warp finishes (host-mapped flag), not when its
- * wave ends. A job whose DP outgrows its arena parks at its current read and
- * is re-admitted with twice the arena. Finished graphs stay resident until
- * released. Results are byte-identical to poa_align_sequences on the same
- * reads, whatever else runs alongside. */
+ * while the server's device pool holds their graph storage, reads, DP arena
+ * and descriptor, and publishes them to the device-side job queue of one
+ * persistent serving kernel: each of its warps (7 per SM) takes the next job
+ * as soon as it finishes its last, so jobs that arrive while others run start
+ * at once on free warps. The kernel ends when its warps have waited idle_ms
+ * without work and is launched again when jobs arrive. A job's completion is
+ * seen as soon as its warp finishes (host-mapped flag). A job whose DP
+ * outgrows its arena parks at its current read and is re-admitted with twice
+ * the arena. Finished graphs stay resident until released. Results are
+ * byte-identical to poa_align_sequences on the same reads, whatever else
+ * runs alongside. */
 typedef struct poa_server poa_server;
 enum {
   POA_SERVER_QUEUED = 0,   /* waiting for admission */
   POA_SERVER_RUNNING = 1,  /* on the device */
   POA_SERVER_DONE = 2,     /* finished; output available until released */
   POA_SERVER_FAILED = 3,   /* finished with an error (poa_server_job_info gives it) */
-  POA_SERVER_PARKED = 4    /* needs a larger DP arena; re-admitted when its wave ends */
+  POA_SERVER_PARKED = 4    /* needs a larger DP arena; re-admitted with twice the arena */
 };
 typedef struct poa_server_job {
   int32_t state;
   int32_t reserved;
   uint64_t cells;      /* band cells computed for the job */
-  double queued_ms;    /* submission to first launch */
+  double queued_ms;    /* submission to admission (published to the kernel's queue) */
   double latency_ms;   /* submission to completion (0 while unfinished) */
 } poa_server_job;
 typedef struct poa_server_stats {
   uint64_t done_jobs;
   uint64_t done_cells;
-  uint64_t waves;          /* kernel launches so far */
+  uint64_t waves;          /* admission rounds published to the serving kernel's queue */
   uint64_t queued;         /* jobs waiting for admission */
-  uint64_t running_waves;
+  uint64_t kernel_launches; /* serving-kernel launches so far */
   uint64_t pool_bytes;
   uint64_t pool_used;
   double busy_s;           /* first submission to the last completion */
 } poa_server_stats;
 /* pool_bytes: device memory of the server (0 = what the context's budget
- * leaves, less 512 MiB); streams: concurrent waves (0 = 64). */
-int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_bytes, int32_t streams,
+ * leaves, less 512 MiB); idle_ms: how long the serving kernel's warps wait
+ * for a job before the kernel ends (0 = 50 ms). */
+int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_bytes, int32_t idle_ms,
                       poa_server **out);
 /* Queues one job (its reads in order); returns at once with its id. */
 int poa_server_submit(poa_ctx *ctx, poa_server *server, int64_t n_seqs, const uint8_t *const *seqs,

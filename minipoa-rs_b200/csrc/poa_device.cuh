@@ -49,6 +49,7 @@ enum Status : int32_t {
   ST_GRAPH_FULL = 101,
   ST_SEEDING_UNSUPPORTED = 102,
   ST_OUT_TOO_SMALL = 103,  // a caller's output buffer holds fewer items than the path
+  ST_WAVE_STALL = 104,     // internal: a row-wavefront step found no row able to advance
 };
 
 __host__ __device__ inline bool is_alignment_error(int32_t s) { return s > 0 && s < 100; }
@@ -66,6 +67,8 @@ struct DevParams {
   int32_t kernel;         // 0 = score-guard dispatch, 1 = i32 only, 2 = i64 only
   int32_t seeding;
   int32_t relaxed_order;  // read loops may keep a spliced order between reads
+  int32_t row_wave;       // static-band int32 rows: 0 one at a time, 1 wavefront where suited, 2 wavefront
+  int32_t byte_prof;      // sigma <= 8 and every score fits a signed byte (dp_wave's packed profile)
   uint64_t b, f;
   uint64_t largest;       // max(|matrix|, |O|, |E|) of i32_scores_safe
 };
@@ -111,7 +114,7 @@ struct Job {
   uint64_t rows_g4;     // rows of the 4-stripe tile (385-512 columns)
   uint64_t rows_generic;  // rows of the generic row (wider bands, many predecessors, i64)
   int32_t coop;         // 1 once a read of the job ran cooperative rows
-  int32_t reserved2;
+  int32_t wave_reads;   // reads whose static-band DP ran as a row wavefront
   uint64_t phase[4];    // profiling builds (POA_PHASE_CYCLES): warp cycles in band guides,
                         // DP rows, traceback, graph update (add_path + rank order)
 };
@@ -122,7 +125,7 @@ struct Job {
 // trip count) and which row paths ran.
 struct Work {
   uint64_t cells, dp_bytes, pred_cells, far_preds, rows_g4, rows_generic;
-  int32_t coop;
+  int32_t coop, wave;
   uint64_t phase[4];
 };
 
@@ -148,6 +151,7 @@ struct Scratch {
   int4 *planc;         // static band, per row: (band start, band length, pred_start, pred_cnt | base << 24)
   int4 *pent;          // static band, per pred entry: where the predecessor's states are (see plan_rows)
   int32_t *nf;         // static band, per row: rows before it that did not go through the ring
+  int4 *wrec;          // row wavefront, per row: an 80-byte record (see plan_wave)
   int32_t *seq;        // encoded, padded query
   uint8_t *seq8;       // the same, one byte per column (when it does not fit shared memory)
   int4 *items;         // alignment result (node, base, aligned, resolved id)
@@ -195,6 +199,7 @@ __device__ inline bool carve_scratch(char *arena, int64_t bytes, int n, int e, i
   s.planc = (int4 *)take(N * 16);
   s.pent = (int4 *)take(int64_t(e + 1) * 16);
   s.nf = (int32_t *)take(N * 4);
+  s.wrec = (int4 *)take(N * 80);
   s.seq = (int32_t *)take((padded + 32) * 4);
   s.seq8 = (uint8_t *)take(padded + 32);
   s.items = (int4 *)take((n_items + 1) * 16);
@@ -594,8 +599,9 @@ __device__ __forceinline__ T mins(T a, T b) {
 // ring so the serial passes read their neighbours without an L2 round trip.
 constexpr int GRING = 32;
 __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int n, int64_t *ring_v,
-                                 int64_t *ring_s) {
+                                 int64_t *ring_s, Work *w) {
   const int lane = threadIdx.x & 31;
+  const uint64_t tg0 = phase_clock();
   int pbase = 0, sbase = 0;
   for (int i0 = 0; i0 < n; i0 += 32) {
     const int i = i0 + lane;
@@ -739,6 +745,10 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
       const Lists cur = nxt;
       nxt = load(st, ct, ent, row_of(q0 + 32 + lane), q0 + 32 + lane < count);
       const int lim = min(32, count - q0);
+      // the block's results stay in the lanes (lane k: row k of the block)
+      // and are stored once at its end, so no row waits behind a store
+      int64_t my_v = 0, my_s = 0;
+      bool my_set = false;
       int lb = __shfl_sync(FULL, cur.start, 0), lc = __shfl_sync(FULL, cur.cnt, 0);
       int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, 0), __shfl_sync(FULL, cur.e0.y, 0));
       int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, 0), __shfl_sync(FULL, cur.e1.y, 0));
@@ -792,9 +802,10 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
         }
         const int64_t vi = have ? bval + 1 : NEG64;
         const int64_t si = have ? bsup + bw : 0;
-        if (have) {
-          val[i] = vi;
-          s.support[i] = si;
+        if (lane == k) {
+          my_v = vi;
+          my_s = si;
+          my_set = have;
         }
         rv[i & (GRING - 1)] = vi;
         rsu[i & (GRING - 1)] = si;
@@ -802,19 +813,31 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
         last_v = vi;
         last_s = si;
       }
+      if (my_set) {
+        const int i = row_of(q0 + lane);
+        val[i] = my_v;
+        s.support[i] = my_s;
+      }
+      __syncwarp();  // later blocks read these rows back from memory
     }
   };
   // forward: head along the heaviest (then most supported) predecessor
+  const uint64_t tg1 = phase_clock();
   s.head[0] = 0;
   rv[0] = 0;
   rsu[0] = 0;
   pass(true, s.head, s.pred_start, s.pred_cnt, s.pred);
+  const uint64_t tg2 = phase_clock();
   // backward: tail along the heaviest (then most supported) successor; the
   // support array continues from the forward pass
   s.tail[n - 1] = 1;
   rv[(n - 1) & (GRING - 1)] = 1;  // rsu keeps the forward support of the last row
   pass(false, s.tail, s.succ_start, s.succ_cnt, s.succ);
   __syncwarp();
+  (void)w;
+  (void)tg0;
+  (void)tg1;
+  (void)tg2;
   return s.head[n - 1] == NEG64 ? ST_NO_PATH : ST_OK;
 }
 
@@ -865,13 +888,15 @@ __device__ inline void adaptive_update(const Job *J, Scratch &s, int beg, int i,
 // preferred-match weight test of the entry's edge, weight >= (sum of the row's
 // incoming weights) / 10 (align.rs:1227-1228). An entry whose predecessor is
 // out of range or skipped has row -1.
-__device__ inline void fill_tb(Scratch &s, int n) {
+__device__ inline int fill_tb(Scratch &s, int n) {
   const int lane = threadIdx.x & 31;
+  int wmax = 0;
   for (int i = lane; i < n; i += 32) {
     const int pb = s.pred_start[i], pc = s.pred_cnt[i];
     const int64_t ws10 = s.wsum[i] / 10;
     for (int t = 0; t < pc; ++t) {
       const int2 pr = s.pred[pb + t];
+      wmax = max(wmax, pr.y);
       int4 a = make_int4(-1, 0, 0, pr.y), b = make_int4(0, 0, 0, 0);
       if (pr.x >= 0) {
         const int p = pr.x;
@@ -886,6 +911,7 @@ __device__ inline void fill_tb(Scratch &s, int n) {
     }
   }
   __syncwarp();
+  return int(__reduce_max_sync(FULL, unsigned(wmax)));
 }
 
 // Traceback of align.rs:1164-1347 by the whole warp, reading the stored DP
@@ -905,14 +931,14 @@ __device__ inline void fill_tb(Scratch &s, int n) {
 // which also reverses them and prepends the source.
 template <typename S>
 __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A, int beg, int n, int64_t m,
-                             const int32_t *mat, const uint8_t *q8, int *n_out) {
+                             const int32_t *mat, const uint8_t *q8, int *n_out, Work *w = nullptr) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
   const int lane = threadIdx.x & 31;
   const int64_t neg_half = int64_t(NEGV) / 2;
   const int64_t O = P.gap_open, E = P.gap_ext;
   constexpr int KIND_INS = 0, KIND_DIAG = 1;
   const int4 none = make_int4(-1, 0, 0, 0), zero = make_int4(0, 0, 0, 0);
-  fill_tb(s, n);
+  const bool small_w = fill_tb(s, n) < (1 << 26);
   int i = n - 1;
   int j = int(m - 1);
   int op = OP_ALL;
@@ -933,6 +959,7 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
   auto eoff = [](const int4 &b) { return int64_t(uint64_t(uint32_t(b.x)) | (uint64_t(uint32_t(b.y) & 0xffffu) << 32)); };
   int32_t st = ST_OK;
   while (i > 0 || j > 0) {
+    const uint64_t ts0 = phase_clock();
     steps += 1;
     if (steps > int64_t(n) + m) {
       st = ST_TB_NO_ADVANCE;
@@ -943,7 +970,16 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
       break;
     }
     // one round of loads: the current cell (and its left neighbour), every
-    // predecessor cell, and the predecessors' first two entries
+    // predecessor cell, and the predecessors' first two entries; each lane
+    // also loads the descriptor of row i - 1 - lane for the L2 prefetch below
+    const int pf_r = i - 1 - lane;
+    int64_t pf_o = 0;
+    int pf_s = 0, pf_l = 0;
+    if (pf_r >= 0) {
+      pf_o = s.row_off[pf_r];
+      pf_s = s.row_start[pf_r];
+      pf_l = s.row_len[pf_r];
+    }
     const int64_t Mij = at(ro, rs, rl, 0, j), Dij = at(ro, rs, rl, 1, j), Iij = at(ro, rs, rl, 2, j);
     const int64_t Mim = at(ro, rs, rl, 0, j - 1), Iim = at(ro, rs, rl, 2, j - 1);
     int64_t Mpm = NEGV, Mpj = NEGV, Dpj = NEGV;
@@ -967,17 +1003,47 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
       st = ST_TB_LEFT_BAND;
       break;
     }
+    // The path reaches the rows just below this one within the next steps,
+    // near this column; their states were written a whole read ago and have
+    // usually left L2, so each lane brings one row's M, D and I around the
+    // column it will likely be reached at back into L2 (descriptors loaded
+    // with this step's states, so issuing costs no wait).
+    if (pf_r >= 0) {
+      const int c0 = max(j - 8 - lane, pf_s), c1 = min(j + 1, pf_s + pf_l - 1);
+      if (c0 <= c1) {
+        const S *base = A + pf_o;
+#pragma unroll
+        for (int plane = 0; plane < 3; ++plane) {
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(base + int64_t(plane) * pf_l + (c0 - pf_s)));
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(base + int64_t(plane) * pf_l + (c1 - pf_s)));
+        }
+      }
+    }
+    const uint64_t ts1 = phase_clock();
     const int qb = q8[j];
     const int64_t score = mat[rb * P.sigma + qb];
     // per-predecessor flags; best lane and weight per kind (chunk 0 from the
     // registers, further chunks of 32 from memory)
     int m_lane = -1, m_w = 0, o_lane = -1, o_w = 0, x_lane = -1, x_w = 0;
     int m_chunk = 0, o_chunk = 0, x_chunk = 0;
+    // one reduction per kind: the key holds a valid bit, the weight and
+    // 31 - lane, so the largest key is the largest weight and, among equal
+    // weights, the first predecessor (weights below 2^26, checked once per
+    // traceback; otherwise a ballot, a maximum and a second ballot)
     auto best = [&](bool f, int w, int t0, int &bl, int &bw, int &bc) {
-      const unsigned msk = __ballot_sync(FULL, f);
-      if (!msk) return;
-      const int mx = __reduce_max_sync(FULL, f ? unsigned(w) : 0u);
-      const int l = __ffs(__ballot_sync(FULL, f && w == mx)) - 1;
+      int l, mx;
+      if (small_w) {
+        const unsigned key = f ? (0x80000000u | (unsigned(w) << 5) | unsigned(31 - lane)) : 0u;
+        const unsigned k = __reduce_max_sync(FULL, key);
+        if (!k) return;
+        l = 31 - int(k & 31u);
+        mx = int((k >> 5) & 0x3ffffffu);
+      } else {
+        const unsigned msk = __ballot_sync(FULL, f);
+        if (!msk) return;
+        mx = int(__reduce_max_sync(FULL, f ? unsigned(w) : 0u));
+        l = __ffs(__ballot_sync(FULL, f && w == mx)) - 1;
+      }
       if (bl < 0 || mx > bw) {
         bl = l;
         bw = mx;
@@ -1013,6 +1079,19 @@ __device__ int32_t traceback(Job *J, const DevParams &P, Scratch &s, const S *A,
       best(fo, qa.w, t0, o_lane, o_w, o_chunk);
       best(fx, qa.w, t0, x_lane, x_w, x_chunk);
     }
+#ifdef POA_PHASE_CYCLES
+    // profiling builds: cycles waiting for the step's loads, cycles choosing
+    // (in the row-path counters, unused by these builds) and steps
+    if (w) {
+      w->rows_g4 += ts1 - ts0;
+      w->rows_generic += phase_clock() - ts1;
+      w->far_preds += 1;
+    }
+#else
+    (void)ts0;
+    (void)ts1;
+    (void)w;
+#endif
     // moves to predecessor (lane l of chunk c): its descriptor becomes the
     // current row, its first two entries come from lane l's prefetch
     auto move_to = [&](int l, int c) {
@@ -1619,6 +1698,328 @@ __device__ __forceinline__ int4 ld_early(const int4 *p) {
   return v;
 }
 
+// ---------------------------------------------------------------------------
+// Row wavefront (static band, int32; align.rs:751-828 for every row at once).
+// With a static band every row's band is known before the DP starts, so the
+// rows need not run one after another: row i may compute its columns
+// [8c, 8c + 8) ("chunk c") as soon as each predecessor has computed its own
+// chunk c (the diagonal also needs the predecessor's column 8c - 1, which
+// belongs to its chunk c - 1). Each lane owns one row at a time (rows
+// 1 + lane, 33 + lane, ...) and walks it chunk by chunk with the serial
+// recurrences in registers; the warp steps in lockstep, so about 32 rows are
+// in flight, each a chunk or more behind the row before it. There is no
+// cross-lane scan: the insertion state I is carried along the row by the
+// lane that owns it.
+//
+// A chunk's M and D, with the M just left of it, go to a shared-memory slot
+// of the lane that computed it (WAVE_KB slots per lane, indexed by chunk mod
+// WAVE_KB) tagged (row << 13 | chunk), and its M, D and I go to the row's
+// arena row as usual. A reader compares the slot's tag with the chunk it
+// needs: equal, the states are there; smaller, the predecessor has not
+// computed the chunk yet and the reader waits for a later step; larger, the
+// slot was reused after the chunk was written, so the chunk is read from the
+// predecessor's arena row. Every step reads first and writes second, with a
+// warp barrier between, so a reader never sees a slot half-written.
+//
+// The arithmetic is the reference's int32 arithmetic term for term: per
+// predecessor over the overlap of the two 8-aligned bands, M[j] gets
+// Mp[j - 1] (NEG32 at the predecessor's first column) and D[j] gets
+// max(Dp[j] + E, Mp[j] + O); then md = max(M + profile, D), I[start] =
+// NEG32, I[j + 1] = max(I[j] + E, md[j] + O), M = max(md, I).
+constexpr int WAVE_KB = 8;              // chunk slots per lane
+constexpr int WAVE_SLOT = 20;           // int32 per slot: M[8], D[8], M left of the chunk, tag, 2 spare
+constexpr int WAVE_TAG = 17;
+constexpr int WAVE_MAX_ROWS = 1 << 18;  // tags hold the row in 18 bits ...
+constexpr int WAVE_MAX_CHUNKS = 1 << 13;  // ... and the chunk in 13
+static_assert(32 * WAVE_KB * WAVE_SLOT * 4 <= 2 * RING_CAP * 4, "wavefront slots must fit the ring arrays");
+
+// Score of query code `code` (0..7) against a row's base, from the row's
+// scores packed as signed bytes (lo: codes 0-3, hi: 4-7): prmt with the
+// sign-replicate selector nibbles yields the sign-extended byte.
+__device__ __forceinline__ int32_t prof_byte(uint32_t lo, uint32_t hi, uint32_t code) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(lo), "r"(hi), "r"(code * 0x1111u + 0x8880u));
+  return int32_t(d);
+}
+
+// Whether a planned static-band read suits the row wavefront. Rows start
+// about len/256 steps apart (8-column chunks, 32 lanes), so a predecessor d
+// rows back was written about d * len / 256 steps before it is read, and the
+// lane slots keep the last WAVE_KB chunks: predecessors further back than
+// that are read from the arena, and in a lockstep warp one such read delays
+// every lane. The wavefront is used when those reads are predicted for
+// fewer than 0.3% of the predecessor chunk reads (graphs of few, shallow
+// branches); otherwise the row-at-a-time loop runs.
+__device__ inline bool wave_suits(const Scratch &s, int n, int64_t cells) {
+  const int lane = threadIdx.x & 31;
+  const int64_t avg = n > 1 ? cells / n : 0;
+  uint64_t all = 0, far = 0;
+  for (int i = 1 + lane; i < n; i += 32) {
+    const int rs = s.row_start[i], rl = s.row_len[i];
+    if (rl <= 0) continue;
+    const int pb = s.pred_start[i], pc = s.pred_cnt[i];
+    for (int t = 0; t < pc; ++t) {
+      const int4 m = s.pmeta[pb + t];
+      if (m.x < 0 || m.z <= 0) continue;
+      const int lo = max(rs, m.y), hi = min(rs + rl, m.y + m.z);
+      if (hi <= lo) continue;
+      const uint64_t ch = uint64_t(hi - lo) >> 3;
+      all += ch;
+      if (int64_t(i - m.x) * avg > int64_t(WAVE_KB - 2) * 256) far += ch;
+    }
+  }
+  for (int d = 16; d; d >>= 1) {
+    all += __shfl_xor_sync(FULL, all, d);
+    far += __shfl_xor_sync(FULL, far, d);
+  }
+  return far * 1000 < all * 3;
+}
+
+// Per row of a wavefront read, an 80-byte record (wrec, five int4):
+// header (band start | band length << 16, arena offset, base | n << 8,
+// pred_start) and the row's first eight predecessors with a non-empty band
+// as (row, first chunk | chunks << 16). All n such predecessors are also
+// listed compactly from pred_start on in `pent` (read as int2), where a lane
+// finds the ninth and later ones.
+constexpr int WAVE_REC = 20;  // int32 per row record
+constexpr int WAVE_REC_PREDS = 8;
+__device__ inline void plan_wave(Scratch &s, int n) {
+  const int lane = threadIdx.x & 31;
+  int2 *list = reinterpret_cast<int2 *>(s.pent);
+  for (int i = lane; i < n; i += 32) {
+    const int pb = s.pred_start[i], pc = s.pred_cnt[i];
+    int32_t *rec = reinterpret_cast<int32_t *>(s.wrec) + WAVE_REC * i;
+    int nv = 0;
+    if (i > 0) {
+      for (int t = 0; t < pc; ++t) {
+        const int4 m = s.pmeta[pb + t];
+        if (m.x < 0 || m.z <= 0) continue;
+        const int2 e = make_int2(m.x, (m.y >> 3) | ((m.z >> 3) << 16));
+        list[pb + nv] = e;
+        if (nv < WAVE_REC_PREDS) reinterpret_cast<int2 *>(rec + 4)[nv] = e;
+        ++nv;
+      }
+    }
+    *reinterpret_cast<int4 *>(rec) =
+        make_int4(s.row_start[i] | (s.row_len[i] << 16), int(s.row_off[i]), s.row_base[i] | (nv << 8), pb);
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ int4 lds4(const int32_t *p) { return *reinterpret_cast<const int4 *>(p); }
+__device__ __forceinline__ void st4(int32_t *p, int32_t a, int32_t b, int32_t c, int32_t d) {
+  *reinterpret_cast<int4 *>(p) = make_int4(a, b, c, d);
+}
+// Asynchronous 16-byte global -> shared copy (cp.async), its commit and the
+// wait for every copy this thread issued.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const uint32_t sa = uint32_t(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Shared memory of a wavefront beside the chunk slots (the query's shared
+// byte copy is not used by it): per lane two row records (the current row's
+// and the next row's, copied ahead with cp.async), then a 64-entry ring of
+// (row, arena offset) of the rows begun most recently.
+constexpr int WAVE_AUX_BYTES = 32 * 2 * WAVE_REC * 4 + 64 * 8;
+static_assert(WAVE_AUX_BYTES <= SEQ_SMEM, "wavefront records must fit the query's shared bytes");
+
+// Rows 1..n-1 of a planned static-band read (row 0 already in the arena).
+// `slots` is the warp's 20 KB of chunk slots, `aux` its WAVE_AUX_BYTES of
+// records, `q8` the query codes (one byte per column, global), `mat` the
+// scoring matrix and, with BYTEPROF, `pk` each base's scores packed as bytes
+// (two words per base). Returns the number of predecessor chunks read from
+// the arena, or UINT32_MAX when a step found no lane able to advance (never
+// expected: the lowest row in flight can always advance; the bound keeps a
+// planning fault from spinning the warp).
+template <bool BYTEPROF>
+__device__ uint32_t dp_wave(const Scratch &s, int n, int32_t *A, const uint8_t *q8, const int32_t *mat, int sigma,
+                            const uint32_t *pk, int32_t E, int32_t O, int32_t *slots, char *aux, Work *w) {
+  const int lane = threadIdx.x & 31;
+  for (int k = lane; k < 32 * WAVE_KB; k += 32) slots[k * WAVE_SLOT + WAVE_TAG] = -1;
+  int2 *const offring = reinterpret_cast<int2 *>(aux + 32 * 2 * WAVE_REC * 4);
+  for (int k = lane; k < 64; k += 32) offring[k] = make_int2(-1, 0);
+  int32_t *const recs = reinterpret_cast<int32_t *>(aux) + lane * 2 * WAVE_REC;
+  const int32_t *const wrec = reinterpret_cast<const int32_t *>(s.wrec);
+  const int2 *const list = reinterpret_cast<const int2 *>(s.pent);
+  int32_t *const mine = slots + lane * WAVE_KB * WAVE_SLOT;
+  // copies row x's record into its buffer (rows alternate between the two)
+  auto fetch = [&](int x) {
+    int32_t *dst = recs + WAVE_REC * (((x - 1) >> 5) & 1);
+    const int32_t *src = wrec + WAVE_REC * x;
+#pragma unroll
+    for (int k = 0; k < WAVE_REC / 4; ++k) cp_async16(dst + 4 * k, src + 4 * k);
+    cp_async_commit();
+  };
+  int r = 1 + lane;
+  if (r < n) fetch(r);
+  int c = 0, cend = 0, start = 0, len = 0, nv = 0, pb = 0;
+  const int32_t *ents = recs;
+  int32_t *R = A;
+  int32_t icarry = NEG32, mleft = NEG32;
+  uint32_t plo = 0, phi = 0;
+  const int32_t *mrow = mat;
+  // takes the lane's next non-empty row (rows r, r + 32, ...): its record
+  // arrived while the row before it ran; the next row's record is fetched
+  auto begin_row = [&]() -> bool {
+    while (r < n) {
+      cp_async_wait_all();
+      const int32_t *rec = recs + WAVE_REC * (((r - 1) >> 5) & 1);
+      const int4 h = lds4(rec);
+      if (r + 32 < n) fetch(r + 32);
+      const uint32_t band = uint32_t(h.x);
+      if ((band >> 16) > 0) {
+        start = int(band & 0xffffu);
+        len = int(band >> 16);
+        R = A + h.y;
+        nv = h.z >> 8;
+        pb = h.w;
+        ents = rec + 4;
+        const int base = h.z & 0xff;
+        c = start >> 3;
+        cend = (start + len) >> 3;
+        icarry = NEG32;
+        mleft = NEG32;
+        if (BYTEPROF) {
+          plo = pk[2 * base];
+          phi = pk[2 * base + 1];
+        } else {
+          mrow = mat + base * sigma;
+        }
+        offring[r & 63] = make_int2(r, h.y);
+        return true;
+      }
+      r += 32;
+    }
+    return false;
+  };
+  bool have = begin_row();
+  __syncwarp();
+  uint32_t far = 0;
+  for (;;) {
+    if (!__any_sync(FULL, have)) break;
+    const uint64_t tp0 = phase_clock();
+    const uint32_t far_before = far;
+    (void)far_before;
+    int32_t Mx[8], Dx[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      Mx[k] = NEG32;
+      Dx[k] = NEG32;
+    }
+    bool ready = have;
+    if (have) {
+      const int j0 = c << 3;
+      for (int t = 0; t < nv; ++t) {
+        const int2 e = t < WAVE_REC_PREDS ? *reinterpret_cast<const int2 *>(ents + 2 * t) : list[pb + t];
+        const int p = e.x;
+        const int p0 = e.y & 0xffff, p1 = p0 + (e.y >> 16);  // the predecessor's chunks [p0, p1)
+        if (c < p0 || c >= p1) continue;
+        int4 m0, m1, d0, d1;
+        int32_t pv;
+        bool got = false;
+        if (p > 0) {
+          const int32_t *sl = slots + (((p - 1) & 31) * WAVE_KB + (c & (WAVE_KB - 1))) * WAVE_SLOT;
+          const int32_t tag = sl[WAVE_TAG], key = (p << 13) | c;
+          if (tag < key) {
+            ready = false;
+            break;
+          }
+          if (tag == key) {
+            m0 = lds4(sl);
+            m1 = lds4(sl + 4);
+            d0 = lds4(sl + 8);
+            d1 = lds4(sl + 12);
+            pv = sl[16];
+            got = true;
+          }
+        }
+        if (!got) {
+          // the predecessor's arena row; its offset from the ring while the
+          // row is among the last 64 begun
+          const int2 oe = offring[p & 63];
+          const int po = oe.x == p ? oe.y : wrec[WAVE_REC * p + 1];
+          const int pl = (e.y >> 16) << 3;
+          const int k = j0 - (p0 << 3);
+          const int32_t *Q = A + po + k;
+          m0 = lds4(Q);
+          m1 = lds4(Q + 4);
+          d0 = lds4(Q + pl);
+          d1 = lds4(Q + pl + 4);
+          pv = k > 0 ? Q[-1] : NEG32;
+          ++far;
+        }
+        if (c == p0) pv = NEG32;
+        const int32_t mp[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+        const int32_t dp[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+        Mx[0] = maxs(Mx[0], pv);
+#pragma unroll
+        for (int k2 = 1; k2 < 8; ++k2) Mx[k2] = maxs(Mx[k2], mp[k2 - 1]);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) Dx[k2] = __viaddmax_s32(dp[k2], E, __viaddmax_s32(mp[k2], O, Dx[k2]));
+      }
+    }
+    if (!__any_sync(FULL, ready)) return UINT32_MAX;
+    const uint64_t tp1 = phase_clock();
+#ifdef POA_PHASE_CYCLES
+    // profiling builds: gather cycles of steps without / with an arena read
+    // (rows_g4 / rows_generic) and the number of steps with one (far_preds)
+    {
+      const bool anyfar = __any_sync(FULL, far != far_before);
+      if (anyfar) {
+        w->rows_generic += tp1 - tp0;
+        w->far_preds += 1;
+      } else {
+        w->rows_g4 += tp1 - tp0;
+      }
+    }
+#endif
+    __syncwarp();
+    if (ready) {
+      const int j0 = c << 3;
+      const uint2 qw = *reinterpret_cast<const uint2 *>(q8 + j0);
+      int32_t Mo[8], Io[8];
+      int32_t I = icarry;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t code = ((k < 4 ? qw.x : qw.y) >> (8 * (k & 3))) & 0xffu;
+        const int32_t prof = BYTEPROF ? prof_byte(plo, phi, code) : mrow[code];
+        const int32_t md = __viaddmax_s32(Mx[k], prof, Dx[k]);
+        Io[k] = I;
+        Mo[k] = maxs(md, I);
+        I = __viaddmax_s32(I, E, md + O);
+      }
+      int32_t *sl = mine + (c & (WAVE_KB - 1)) * WAVE_SLOT;
+      st4(sl, Mo[0], Mo[1], Mo[2], Mo[3]);
+      st4(sl + 4, Mo[4], Mo[5], Mo[6], Mo[7]);
+      st4(sl + 8, Dx[0], Dx[1], Dx[2], Dx[3]);
+      st4(sl + 12, Dx[4], Dx[5], Dx[6], Dx[7]);
+      sl[16] = mleft;
+      sl[WAVE_TAG] = (r << 13) | c;
+      const int o = j0 - start;
+      st4(R + o, Mo[0], Mo[1], Mo[2], Mo[3]);
+      st4(R + o + 4, Mo[4], Mo[5], Mo[6], Mo[7]);
+      st4(R + len + o, Dx[0], Dx[1], Dx[2], Dx[3]);
+      st4(R + len + o + 4, Dx[4], Dx[5], Dx[6], Dx[7]);
+      st4(R + 2 * len + o, Io[0], Io[1], Io[2], Io[3]);
+      st4(R + 2 * len + o + 4, Io[4], Io[5], Io[6], Io[7]);
+      icarry = I;
+      mleft = Mo[7];
+      if (++c == cend) {
+        r += 32;
+        have = begin_row();
+      }
+    }
+    __syncwarp();
+    (void)tp0;
+    (void)tp1;
+  }
+  cp_async_wait_all();  // no copy outlives the read (the records' memory is reused)
+  return __reduce_add_sync(FULL, far);
+}
+
 // Static-band row plan (warp-wide), after fill_pmeta. Per row (planc):
 // band start and length, predecessor list start and count, and the base
 // code it scores with. Per predecessor entry (pent), where the predecessor's
@@ -1677,9 +2078,11 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w)
     gen += __shfl_xor_sync(FULL, gen, d);
     far += __shfl_xor_sync(FULL, far, d);
   }
+#ifndef POA_PHASE_CYCLES
   w->rows_g4 += g4;
   w->rows_generic += gen;
   w->far_preds += far;
+#endif
 }
 
 // Predecessor-cell updates of a planned read (after fill_pmeta): the sum
@@ -1743,6 +2146,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     const int code = (c == 0 || c > qlen) ? P.unknown : int(P.encode[query[c - 1]]);
     if (c < padded) s.seq[c] = code;
     q8[c] = uint8_t(code);
+    if (q8 != s.seq8) s.seq8[c] = uint8_t(code);  // the row wavefront reads the global copy
   }
   const bool adaptive = adaptive_arg || P.adaptive;
   uint64_t bandu = band_b + (f == 0 ? 0 : uint64_t(m) / f);
@@ -1752,7 +2156,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   const S s00 = S(P.matrix[P.unknown * P.sigma + P.unknown]);
   __syncwarp();
   const uint64_t t_g0 = phase_clock();
-  int32_t st = guides(J, s, beg, end, n, sm ? sm->gring_v : nullptr, sm ? sm->gring_s : nullptr);
+  int32_t st = guides(J, s, beg, end, n, sm ? sm->gring_v : nullptr, sm ? sm->gring_s : nullptr, cells);
   const uint64_t t_g1 = phase_clock();
   cells->phase[0] += t_g1 - t_g0;
   if (st != ST_OK) return st;
@@ -1850,6 +2254,51 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     __syncwarp();
     fill_pmeta(s, n);
     const bool ring = kFastType && sm;
+    if constexpr (kFastType) {
+      // the row wavefront, unless this warp leads cooperative rows (its
+      // helpers wait for rows) or the sizes exceed its tags
+      const bool wave = ring && P.row_wave && sm->rv.pad[0] == 0 && n < WAVE_MAX_ROWS &&
+                        (padded >> 3) < WAVE_MAX_CHUNKS && tot <= INT32_MAX &&
+                        (P.row_wave == 2 || wave_suits(s, n, tot / 3));
+      if (wave) {
+        plan_wave(s, n);
+        cells->pred_cells += pred_overlap_cells(s, n);
+        if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
+        const int32_t *mat = smem_matrix ? sm->matrix : P.matrix;
+        uint32_t far;
+        if (P.byte_prof) {
+          // each base's scores as signed bytes, two words per base
+          uint32_t *pk = reinterpret_cast<uint32_t *>(sm->matrix) + (SMEM_MATRIX - 16);
+          if (lane < 2 * P.sigma) {
+            const int b = lane >> 1, k0 = 4 * (lane & 1);
+            uint32_t w = 0;
+            for (int k = 0; k < 4; ++k)
+              if (k0 + k < P.sigma) w |= (uint32_t(P.matrix[b * P.sigma + k0 + k]) & 0xffu) << (8 * k);
+            pk[lane] = w;
+          }
+          __syncwarp();
+          far = dp_wave<true>(s, n, reinterpret_cast<int32_t *>(A), s.seq8, mat, P.sigma, pk, int32_t(E),
+                              int32_t(O), sm->ring_m, reinterpret_cast<char *>(sm->seq8), cells);
+        } else {
+          __syncwarp();
+          far = dp_wave<false>(s, n, reinterpret_cast<int32_t *>(A), s.seq8, mat, P.sigma, nullptr, int32_t(E),
+                               int32_t(O), sm->ring_m, reinterpret_cast<char *>(sm->seq8), cells);
+        }
+        if (far == UINT32_MAX) return ST_WAVE_STALL;
+        cells->wave = 1;
+#ifndef POA_PHASE_CYCLES
+        cells->far_preds += far;
+#endif
+        cells->cells += row_cells;
+        cells->dp_bytes += row_cells * 3 * sizeof(S);
+        const uint64_t t_w1 = phase_clock();
+        cells->phase[1] += t_w1 - t_g1;
+        // (the query's shared bytes held the wavefront's row records)
+        st = traceback<S>(J, P, s, A, beg, n, m, smem_matrix ? sm->matrix : P.matrix, s.seq8, n_items, cells);
+        cells->phase[2] += phase_clock() - t_w1;
+        return st;
+      }
+    }
     plan_rows(s, n, ring, rcap, cells);
     cells->pred_cells += pred_overlap_cells(s, n);
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
@@ -2071,7 +2520,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   }
   const uint64_t t_d1 = phase_clock();
   cells->phase[1] += t_d1 - t_g1;
-  st = traceback<S>(J, P, s, A, beg, n, m, (sm && smem_matrix) ? sm->matrix : P.matrix, q8, n_items);
+  st = traceback<S>(J, P, s, A, beg, n, m, (sm && smem_matrix) ? sm->matrix : P.matrix, q8, n_items, cells);
   cells->phase[2] += phase_clock() - t_d1;
   return st;
 }
@@ -2388,6 +2837,7 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
       J->rows_g4 += cells.rows_g4;
       J->rows_generic += cells.rows_generic;
       J->coop |= cells.coop;
+      J->wave_reads += cells.wave;
       cells.phase[3] += phase_clock() - t_u0;
       for (int k = 0; k < 4; ++k) J->phase[k] += cells.phase[k];
       J->next_read = r + 1;

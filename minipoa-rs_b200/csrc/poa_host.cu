@@ -69,6 +69,7 @@ std::string status_message(int32_t st, int err_i, int err_j) {
     case ST_GRAPH_FULL: return "graph capacity exhausted";
     case ST_OUT_TOO_SMALL: return "output buffer holds fewer items than the alignment path";
     case ST_SEEDING_UNSUPPORTED: return "seeded windows (-S) are not available in this build";
+    case ST_WAVE_STALL: return "DP row wavefront made no progress (internal error)";
     default: return "unknown device status " + std::to_string(st);
   }
 }
@@ -77,6 +78,7 @@ int status_code(int32_t st) {
   if (is_alignment_error(st)) return POA_ERR_ALIGN;
   if (st == ST_SEEDING_UNSUPPORTED) return POA_ERR_UNSUPPORTED;
   if (st == ST_OUT_TOO_SMALL) return POA_ERR_INVALID;
+  if (st == ST_WAVE_STALL) return POA_ERR_TIMEOUT;
   return POA_ERR_ALLOC;
 }
 
@@ -164,7 +166,13 @@ char *dup_string(const std::string &s) {
 
 // ---------------------------------------------------------------------------
 
+struct poa_batch;
+
 struct poa_ctx {
+  // live batches of this context: a batch that needs its DP arena pool while
+  // others hold theirs takes their memory back (they re-allocate on their
+  // next run)
+  std::vector<poa_batch *> batches;
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -258,6 +266,16 @@ struct poa_ctx {
     P.kernel = 0;
     P.seeding = hp.seeding ? 1 : 0;
     P.relaxed_order = 1;  // read loops finish with the exact LIFO order
+    // static-band int32 rows: row at a time (0, the default: measured
+    // fastest on the benchmark's mixed batch), as a wavefront where a read
+    // suits it (MINIPOA_DP_ROWS=auto) or always (=wave)
+    const char *rows_env = std::getenv("MINIPOA_DP_ROWS");
+    P.row_wave = 0;
+    if (rows_env && std::strcmp(rows_env, "auto") == 0) P.row_wave = 1;
+    if (rows_env && std::strcmp(rows_env, "wave") == 0) P.row_wave = 2;
+    P.byte_prof = P.sigma <= 8 ? 1 : 0;
+    for (int32_t v : hp.matrix)
+      if (v < -128 || v > 127) P.byte_prof = 0;
     P.b = hp.b;
     P.f = hp.f;
     P.largest = hp.largest();
@@ -889,9 +907,20 @@ struct poa_batch {
   size_t order_bytes() const { return 2 * order_half() * 4; }
   int32_t *base_order() const { return d_order + order_half(); }
 
+  // Frees the DP arena pool (and the captured run that points into it).
+  void drop_arenas() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    g_slots = g_slot_bytes = -1;
+    if (ctx) ctx->dfree(arenas, size_t(arena_pool));
+    arenas = nullptr;
+    arena_pool = 0;
+  }
+
   ~poa_batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (!ctx) return;
+    ctx->batches.erase(std::remove(ctx->batches.begin(), ctx->batches.end(), this), ctx->batches.end());
     ctx->dfree(d_read_off, reads_bytes);  // base of the reads allocation
     ctx->dfree(d_matrix, 0);
     ctx->dfree(d_encode, 0);
@@ -1549,6 +1578,7 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     CK(cudaEventCreate(&b->k0));
     CK(cudaEventCreate(&b->k1));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->batches.push_back(b.get());
     *out = b.release();
   });
 }
@@ -1617,6 +1647,9 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
     if (mode != 0 && mode != 1) throw AlignError{POA_ERR_INVALID, "mode must be 0 (batched) or 1 (plain)"};
     // arena pool: the rest of the budget, allocated once
     if (!b->arenas) {
+      // the other batches' pools are idle between their runs: take them back
+      for (poa_batch *o : ctx->batches)
+        if (o != b && o->arenas) o->drop_arenas();
       const uint64_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
       const int64_t pool = int64_t(left) - (int64_t(256) << 20);
       if (pool < (int64_t(64) << 20)) throw AlignError{POA_ERR_ALLOC, "no device memory left for DP arenas"};
@@ -1727,7 +1760,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
     if (stats) {
       for (int k = 0; k < 4; ++k) stats->phase_cycles[k] = 0;
       uint64_t cells = 0, reads = 0, dpb = 0, pc = 0, far = 0, g4 = 0, gen = 0;
-      int32_t coop = 0;
+      int32_t coop = 0, wave = 0;
       for (auto &J : b->jobs) {
         cells += J.cells;
         dpb += J.dp_bytes;
@@ -1737,6 +1770,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
         g4 += J.rows_g4;
         gen += J.rows_generic;
         coop += J.coop;
+        wave += J.wave_reads;
         for (int k = 0; k < 4; ++k) stats->phase_cycles[k] += J.phase[k];
       }
       stats->cells = cells;
@@ -1746,7 +1780,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
       stats->rows_g4 = g4;
       stats->rows_generic = gen;
       stats->coop_jobs = coop;
-      stats->reserved2 = 0;
+      stats->wave_reads = wave;
       stats->kernel_ms = kernel_ms;
       stats->reads = reads;
       stats->device_ms = ms;
@@ -1897,11 +1931,13 @@ void poa_batch_free(poa_batch *batch) { delete batch; }
 
 // ---------------------------------------------------------------------------
 // Serving loop: continuous batching of independent jobs (read sets, optionally
-// extending a graph built from earlier reads). Jobs are admitted in arrival
-// order while the server's device pool holds their graph storage, reads and
-// DP arena; every admission round launches the admitted jobs as one wave of
-// the batched kernel on its own stream, so waves that arrive while others run
-// overlap on the device. Finished graphs stay resident until released.
+// extending a graph built from earlier reads). A dispatcher thread admits
+// jobs in arrival order while the server's device pool holds their graph
+// storage, reads, DP arena and descriptor, and publishes them to the job
+// queue of one persistent serving kernel (k_serve), whose warps take jobs as
+// they free up; the kernel ends after its warps have been idle a while and
+// is launched again when work arrives. Finished graphs stay resident until
+// released.
 
 namespace {
 
@@ -1963,13 +1999,14 @@ struct ServerJob {
   // get sequence ids after its `existing` path records
   std::unique_ptr<BuildGraph> init;
   std::vector<int32_t> init_rank, init_order;
+  std::unique_ptr<GraphImage> image;  // the initial graph's device arrays, built by the submitting thread
   int32_t existing = 0;
   int skips = 0;  // admission rounds that passed this job over at the head of the queue
   Caps caps;
   uint64_t storage_bytes = 0, reads_bytes = 0, arena_bytes = 0;
   char *storage = nullptr, *reads = nullptr, *arena = nullptr;
   Job J{};  // host copy of the device descriptor
-  Job *d_desc = nullptr;  // its device copy while a wave runs it
+  Job *d_desc = nullptr;  // its device copy (in the pool) while it is admitted
   int done_slot = -1;     // host-mapped flag the kernel raises when the job leaves it
   bool fresh = true;
   int32_t state = POA_SERVER_QUEUED;
@@ -1977,13 +2014,13 @@ struct ServerJob {
   double t_submit = 0, t_start = 0, t_done = 0;
 };
 
-struct Wave {
-  int stream = 0;
-  cudaEvent_t done = nullptr;
-  std::vector<int64_t> ids;
-  char *mem = nullptr;
-  uint64_t mem_bytes = 0;
-  Job *d_jobs = nullptr;
+// Pinned staging of one admission round (reads, descriptors, queue entries
+// and the new tail), reusable once the round's copies have completed.
+struct Stage {
+  char *p = nullptr;
+  size_t cap = 0;
+  cudaEvent_t ev = nullptr;
+  bool used = false;
 };
 
 }  // namespace
@@ -1999,13 +2036,18 @@ struct poa_server {
   std::condition_variable cv;
   std::map<int64_t, std::unique_ptr<ServerJob>> jobs;
   std::deque<int64_t> pending;
-  std::vector<Wave> waves;
-  std::vector<cudaStream_t> streams;
-  std::vector<int> free_streams;
-  // pinned staging of the reads a wave uploads, one buffer per stream slot
-  // (reused once the slot's wave has finished, so no copy waits on the host)
-  std::vector<char *> stage;
-  std::vector<size_t> stage_bytes;
+  // the persistent serving kernel and its job queue (device memory, in the
+  // pool); uploads and queue publication go in order on up_stream
+  ServeQueue *d_q = nullptr;
+  uint32_t tail = 0;            // queue entries published
+  uint32_t head_seen = 0;       // entries claimed, as last read while no kernel ran
+  cudaStream_t up_stream = nullptr, k_stream = nullptr;
+  cudaEvent_t k_done = nullptr;
+  bool k_live = false;          // a serving kernel was launched and has not been seen to end
+  bool stopping = false;        // its stop flag is set (the server was idle)
+  int64_t idle_ns = 50000000;   // the kernel ends after the server has been idle this long
+  double last_busy = 0;         // when the server last had queued or running jobs
+  std::vector<Stage> stages;
   cudaStream_t out_stream = nullptr;
   std::thread worker;
   bool stop = false;
@@ -2017,7 +2059,7 @@ struct poa_server {
   std::string fatal;
   double arena_scale = 1.0;  // multiplies the first DP arena of each job
   // statistics of finished jobs
-  uint64_t done_jobs = 0, done_cells = 0, launched_waves = 0;
+  uint64_t done_jobs = 0, done_cells = 0, rounds = 0, launches = 0;
   double first_submit = -1, last_done = 0;
 
   ~poa_server() {
@@ -2027,13 +2069,26 @@ struct poa_server {
     }
     cv.notify_all();
     if (worker.joinable()) worker.join();
-    for (auto &w : waves) {
-      cudaEventSynchronize(w.done);
-      cudaEventDestroy(w.done);
+    // the worker leaves with the queue empty and every job done; a kernel
+    // still polling sees stop and leaves
+    if (d_q && up_stream) {
+      static const uint32_t leave = 2;
+      cudaMemcpyAsync(&d_q->stop, &leave, 4, cudaMemcpyHostToDevice, up_stream);
+      cudaStreamSynchronize(up_stream);
     }
-    for (auto st : streams) cudaStreamDestroy(st);
-    for (char *p : stage)
-      if (p) cudaFreeHost(p);
+    if (k_done) {
+      if (k_live) cudaEventSynchronize(k_done);
+      cudaEventDestroy(k_done);
+    }
+    for (auto &st : stages) {
+      if (st.ev) {
+        cudaEventSynchronize(st.ev);
+        cudaEventDestroy(st.ev);
+      }
+      if (st.p) cudaFreeHost(st.p);
+    }
+    if (up_stream) cudaStreamDestroy(up_stream);
+    if (k_stream) cudaStreamDestroy(k_stream);
     if (out_stream) cudaStreamDestroy(out_stream);
     if (h_done) cudaFreeHost(h_done);
     if (ctx) ctx->dfree(pool_mem, pool_bytes);
@@ -2074,14 +2129,16 @@ struct poa_server {
   }
 
   void run();
-  void finish_wave(Wave &w);
   bool finish_jobs();
-  bool launch_wave();
+  bool admit_jobs();
+  bool keep_kernel();
+  Stage &stage_for(size_t need);
 };
 
-// Jobs whose completion flag is up: their descriptor is read back and their
-// arena and reads go back to the pool while the rest of the wave runs. Parked
-// jobs (arena too small) are requeued when their wave ends.
+// Jobs whose completion flag is up: their descriptor is read back, and their
+// arena, reads and descriptor go back to the pool while the other jobs run.
+// A parked job (arena too small) goes back to the head of the queue with
+// twice the arena; its graph stays where it is.
 bool poa_server::finish_jobs() {
   std::vector<int64_t> ready;
   {
@@ -2107,14 +2164,21 @@ bool poa_server::finish_jobs() {
     running.erase(std::find(running.begin(), running.end(), id));
     free_done.push_back(sj.done_slot);
     sj.done_slot = -1;
+    pool.give(reinterpret_cast<char *>(sj.d_desc), sizeof(Job));
+    sj.d_desc = nullptr;
     sj.J = hj;
+    pool.give(sj.arena, sj.arena_bytes);
+    sj.arena = nullptr;
     if (hj.status == ST_ARENA_FULL) {
-      sj.state = POA_SERVER_PARKED;
+      sj.arena_bytes *= 2;
+      sj.J.status = ST_OK;
+      sj.fresh = false;
+      sj.state = POA_SERVER_QUEUED;
+      pending.push_front(sj.id);
       continue;
     }
-    pool.give(sj.arena, sj.arena_bytes);
     pool.give(sj.reads, sj.reads_bytes);
-    sj.arena = sj.reads = nullptr;
+    sj.reads = nullptr;
     sj.t_done = t;
     if (hj.status == ST_OK) {
       sj.state = POA_SERVER_DONE;
@@ -2130,56 +2194,72 @@ bool poa_server::finish_jobs() {
   return true;
 }
 
-void poa_server::finish_wave(Wave &w) {
-  finish_jobs();  // flags raised just before the wave ended
-  std::lock_guard<std::mutex> lk(mu);
-  for (int64_t id : w.ids) {
-    auto it = jobs.find(id);
-    if (it == jobs.end()) continue;  // finished early and already released by its caller
-    ServerJob &sj = *it->second;
-    sj.d_desc = nullptr;
-    if (sj.state != POA_SERVER_PARKED) continue;
-    // the graph is intact at its next read; come back with twice the arena
-    pool.give(sj.arena, sj.arena_bytes);
-    sj.arena = nullptr;
-    sj.arena_bytes *= 2;
-    sj.J.status = ST_OK;
-    sj.fresh = false;
-    sj.state = POA_SERVER_QUEUED;
-    pending.push_front(sj.id);
+// A pinned staging buffer of at least `need` bytes whose earlier copies have
+// completed (waiting for the oldest one when all are in flight).
+Stage &poa_server::stage_for(size_t need) {
+  for (;;) {
+    Stage *pick = nullptr;
+    for (auto &st : stages) {
+      if (st.used) {
+        const cudaError_t q = cudaEventQuery(st.ev);
+        if (q == cudaErrorNotReady) {
+          cudaGetLastError();  // not an error: the copies are still running
+          continue;
+        }
+        CK(q);
+      }
+      pick = &st;
+      break;
+    }
+    if (!pick) {
+      CK(cudaEventSynchronize(stages.front().ev));
+      std::rotate(stages.begin(), stages.begin() + 1, stages.end());
+      continue;
+    }
+    if (pick->cap < need) {
+      if (pick->p) CK(cudaFreeHost(pick->p));
+      pick->p = nullptr;
+      pick->cap = 0;
+      const size_t cap = std::max<size_t>(need, size_t(1) << 20);
+      CK(cudaHostAlloc(reinterpret_cast<void **>(&pick->p), cap, cudaHostAllocDefault));
+      pick->cap = cap;
+    }
+    if (!pick->ev) CK(cudaEventCreateWithFlags(&pick->ev, cudaEventDisableTiming));
+    pick->used = true;
+    return *pick;
   }
-  pool.give(w.mem, w.mem_bytes);
-  free_streams.push_back(w.stream);
-  cudaEventDestroy(w.done);
-  cv.notify_all();
 }
 
-// Admits queued jobs in arrival order while the pool holds them and launches
-// them as one wave; returns whether a wave was launched.
-bool poa_server::launch_wave() {
-  Wave w;
+// Admits queued jobs in arrival order while the pool holds their graph
+// storage, reads, DP arena and descriptor, uploads them and publishes them
+// to the serving kernel's queue; returns whether any job was admitted.
+bool poa_server::admit_jobs() {
   std::vector<ServerJob *> adm;
   {
     std::lock_guard<std::mutex> lk(mu);
-    if (pending.empty() || free_streams.empty()) return false;
-    // Admission in arrival order, looking past a job that does not fit into
-    // the free pool for up to kLookahead later jobs that do; a head job
-    // passed over kMaxSkips times holds back the jobs behind it, so a large
-    // job is not starved by a stream of small ones.
+    if (pending.empty()) return false;
+    // Arrival order, looking past a job that does not fit into the free pool
+    // for up to kLookahead later jobs that do; a head job passed over
+    // kMaxSkips times holds back the jobs behind it, so a large job is not
+    // starved by a stream of small ones.
     constexpr int kLookahead = 32, kMaxSkips = 8;
     int passed = 0;
-    for (size_t pi = 0; pi < pending.size() && adm.size() < free_done.size();) {
+    for (size_t pi = 0; pi < pending.size() && adm.size() < free_done.size() &&
+                        running.size() + adm.size() + 1 < size_t(SERVE_QCAP);) {
       ServerJob &sj = *jobs.at(pending[pi]);
       char *st = sj.storage ? sj.storage : pool.take(sj.storage_bytes);
       char *rd = sj.reads ? sj.reads : (st ? pool.take(sj.reads_bytes) : nullptr);
       char *ar = (st && rd) ? pool.take(sj.arena_bytes) : nullptr;
-      if (!ar) {
+      char *ds = ar ? pool.take(sizeof(Job)) : nullptr;
+      if (!ds) {
+        pool.give(ar, sj.arena_bytes);
         if (!sj.storage) pool.give(st, sj.storage_bytes);
         if (!sj.reads) pool.give(rd, sj.reads_bytes);
         // a job larger than the whole idle pool can never run
-        if (waves.empty() && adm.empty()) {
+        if (running.empty() && adm.empty()) {
+          pool.give(sj.storage, sj.storage_bytes);
           pool.give(sj.reads, sj.reads_bytes);
-          sj.reads = nullptr;
+          sj.storage = sj.reads = nullptr;
           sj.state = POA_SERVER_FAILED;
           sj.error = "job needs more device memory than the server pool";
           sj.t_done = now_s();
@@ -2195,57 +2275,41 @@ bool poa_server::launch_wave() {
       sj.storage = st;
       sj.reads = rd;
       sj.arena = ar;
+      sj.d_desc = reinterpret_cast<Job *>(ds);
       pending.erase(pending.begin() + long(pi));
       adm.push_back(&sj);
     }
     if (adm.empty()) return false;
-    w.mem_bytes = adm.size() * sizeof(Job) + sched_words(adm.size()) * 4 + adm.size() * 4 + 1024;
-    w.mem = pool.take(w.mem_bytes);
-    if (!w.mem) {
-      for (auto it = adm.rbegin(); it != adm.rend(); ++it) {
-        pool.give((*it)->arena, (*it)->arena_bytes);
-        (*it)->arena = nullptr;
-        pending.push_front((*it)->id);
-      }
-      return false;
-    }
-    w.stream = free_streams.back();
-    free_streams.pop_back();
   }
-  // fresh jobs without an initial graph first (they are reset to
-  // Graph::new), then fresh jobs with one (their graph is copied in), then
-  // parked ones, which keep their graph
-  std::stable_partition(adm.begin(), adm.end(), [](const ServerJob *j) { return j->fresh; });
-  std::stable_partition(adm.begin(), adm.end(), [](const ServerJob *j) { return j->fresh && !j->init; });
-  const cudaStream_t stream = streams[size_t(w.stream)];
+  // fresh jobs are uploaded (reads; an initial graph is copied in), every
+  // admitted job's descriptor goes to its place in the pool, then the queue
+  // entries and the new tail: all in order on up_stream, from one pinned
+  // staging buffer
   const double t = now_s();
-  std::vector<Job> hj(adm.size());
-  int n_fresh = 0;
-  size_t need = adm.size() * (sizeof(Job) + 4) + 256;  // descriptors and queue
+  size_t need = adm.size() * (PoolAlloc::round(sizeof(Job)) + 8) + 64;
   for (ServerJob *j : adm)
-    if (j->fresh) need += (j->reads_bytes + 255) / 256 * 256;
-  if (stage_bytes[size_t(w.stream)] < need) {
-    if (stage[size_t(w.stream)]) cudaFreeHost(stage[size_t(w.stream)]);
-    stage[size_t(w.stream)] = nullptr;
-    stage_bytes[size_t(w.stream)] = 0;
-    CK(cudaHostAlloc(reinterpret_cast<void **>(&stage[size_t(w.stream)]), need, cudaHostAllocDefault));
-    stage_bytes[size_t(w.stream)] = need;
-  }
-  char *staging = stage[size_t(w.stream)];
+    if (j->fresh) need += PoolAlloc::round(j->reads_bytes);
+  Stage &stg = stage_for(need);
+  char *staging = stg.p;
   size_t staged = 0;
-  for (size_t k = 0; k < adm.size(); ++k) {
-    ServerJob &sj = *adm[k];
+  std::vector<unsigned long long> entries;
+  entries.reserve(adm.size());
+  for (ServerJob *jp : adm) {
+    ServerJob &sj = *jp;
+    bool reset = false;
     if (sj.fresh) {
-      if (!sj.init) ++n_fresh;
       Job J{};
       layout(sj.caps, sj.storage, &J);
       if (sj.init) {
-        // the initial graph, ranked in the reference's LIFO order
-        const GraphImage img = graph_image(*sj.init, sj.caps, &sj.init_rank, &sj.init_order);
-        put_image(img, sj.caps, J, stream);
-        CK(cudaStreamSynchronize(stream));  // the image goes out of scope
+        // the initial graph, ranked in the reference's LIFO order; copies
+        // from pageable memory return once the driver has staged the bytes,
+        // so the image can go at once
+        put_image(*sj.image, sj.caps, J, up_stream);
+        sj.image.reset();
         J.order_exact = 1;
         J.seq_base = sj.existing;
+      } else {
+        reset = true;  // Graph::new on the device when a warp takes the job
       }
       const int64_t n = int64_t(sj.lens.size());
       J.read_off = reinterpret_cast<int64_t *>(sj.reads);
@@ -2253,7 +2317,7 @@ bool poa_server::launch_wave() {
       J.reads = reinterpret_cast<uint8_t *>(sj.reads + n * 12);
       J.n_reads = int32_t(n);
       char *host = staging + staged;
-      staged += (sj.reads_bytes + 255) / 256 * 256;
+      staged += PoolAlloc::round(sj.reads_bytes);
       std::memset(host, 0, sj.reads_bytes);
       int64_t at = 0;
       for (int64_t r = 0; r < n; ++r) {
@@ -2262,7 +2326,7 @@ bool poa_server::launch_wave() {
         at += sj.lens[size_t(r)];
       }
       if (!sj.bytes.empty()) std::memcpy(host + n * 12, sj.bytes.data(), sj.bytes.size());
-      CK(cudaMemcpyAsync(sj.reads, host, sj.reads_bytes, cudaMemcpyHostToDevice, stream));
+      CK(cudaMemcpyAsync(sj.reads, host, sj.reads_bytes, cudaMemcpyHostToDevice, up_stream));
       sj.J = J;
       sj.t_start = t;
     }
@@ -2277,51 +2341,68 @@ bool poa_server::launch_wave() {
     h_done[sj.done_slot] = 0;
     sj.J.done_flag = d_done + sj.done_slot;
     sj.state = POA_SERVER_RUNNING;
-    hj[k] = sj.J;
-    w.ids.push_back(sj.id);
+    std::memcpy(staging + staged, &sj.J, sizeof(Job));
+    CK(cudaMemcpyAsync(sj.d_desc, staging + staged, sizeof(Job), cudaMemcpyHostToDevice, up_stream));
+    staged += PoolAlloc::round(sizeof(Job));
+    entries.push_back(reinterpret_cast<unsigned long long>(sj.d_desc) | (reset ? 1ull : 0ull));
   }
-  char *m = w.mem;
-  w.d_jobs = reinterpret_cast<Job *>(m);
-  int32_t *d_order = reinterpret_cast<int32_t *>(m + PoolAlloc::round(hj.size() * sizeof(Job)));
-  int32_t *d_sched = d_order + (hj.size() + 63) / 64 * 64;
-  // the wave's queue: largest estimated work first
-  std::vector<int32_t> order(hj.size());
-  std::iota(order.begin(), order.end(), 0);
-  std::vector<double> work(adm.size());
-  for (size_t k = 0; k < adm.size(); ++k) {
-    double sum = 0;
-    for (int64_t l : adm[k]->lens) sum += double(l);
-    work[k] = sum * double(first_arena(*adm[k]));
-  }
-  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return work[size_t(a)] > work[size_t(c)]; });
-  // descriptors and queue through the wave's pinned staging (after the reads)
-  const size_t jb = hj.size() * sizeof(Job), ob = order.size() * 4;
-  if (staged + jb + ob > stage_bytes[size_t(w.stream)]) {
-    CK(cudaStreamSynchronize(stream));  // the reads already staged are in flight
-    if (stage[size_t(w.stream)]) cudaFreeHost(stage[size_t(w.stream)]);
-    stage[size_t(w.stream)] = nullptr;
-    stage_bytes[size_t(w.stream)] = 0;
-    CK(cudaHostAlloc(reinterpret_cast<void **>(&stage[size_t(w.stream)]), jb + ob + 256, cudaHostAllocDefault));
-    stage_bytes[size_t(w.stream)] = jb + ob + 256;
-    staging = stage[size_t(w.stream)];
-    staged = 0;
-  }
-  std::memcpy(staging + staged, hj.data(), jb);
-  std::memcpy(staging + staged + jb, order.data(), ob);
-  CK(cudaMemcpyAsync(w.d_jobs, staging + staged, jb, cudaMemcpyHostToDevice, stream));
-  CK(cudaMemcpyAsync(d_order, staging + staged + jb, ob, cudaMemcpyHostToDevice, stream));
-  CK(cudaMemsetAsync(d_sched, 0, sched_words(hj.size()) * 4, stream));
-  if (n_fresh) CK(launch_reset(w.d_jobs, n_fresh, P.sigma, P.unknown, stream));
-  CK(launch_batch(w.d_jobs, d_order, int(hj.size()), d_sched, ctx->sm_count, P, nullptr, 0, int(hj.size()), stream));
-  CK(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
-  CK(cudaEventRecord(w.done, stream));
+  // queue entries (split where the ring wraps), then the tail
+  unsigned long long *ent = reinterpret_cast<unsigned long long *>(staging + staged);
+  std::memcpy(ent, entries.data(), entries.size() * 8);
+  staged += entries.size() * 8;
+  const uint32_t first = tail % SERVE_QCAP;
+  const size_t n1 = std::min<size_t>(entries.size(), size_t(SERVE_QCAP - first));
+  CK(cudaMemcpyAsync(&d_q->slot[first], ent, n1 * 8, cudaMemcpyHostToDevice, up_stream));
+  if (n1 < entries.size())
+    CK(cudaMemcpyAsync(&d_q->slot[0], ent + n1, (entries.size() - n1) * 8, cudaMemcpyHostToDevice, up_stream));
+  uint32_t *new_tail = reinterpret_cast<uint32_t *>(staging + staged);
+  *new_tail = tail + uint32_t(entries.size());
+  CK(cudaMemcpyAsync(&d_q->tail, new_tail, 4, cudaMemcpyHostToDevice, up_stream));
+  CK(cudaEventRecord(stg.ev, up_stream));
+  tail += uint32_t(entries.size());
   std::lock_guard<std::mutex> lk(mu);
-  for (size_t k = 0; k < adm.size(); ++k) {
-    adm[k]->d_desc = w.d_jobs + k;
-    running.push_back(adm[k]->id);
+  for (ServerJob *jp : adm) running.push_back(jp->id);
+  ++rounds;
+  return true;
+}
+
+// Keeps the serving kernel running while the server has work, and ends it
+// (stop = 1: its warps leave once the queue is empty) after idle_ns without
+// any; a kernel that ended with entries still unclaimed (published as it
+// stopped) is launched again, with stop cleared first.
+bool poa_server::keep_kernel() {
+  static const uint32_t kRun = 0, kStop = 1;
+  const double t = now_s();
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pending.empty() || !running.empty()) last_busy = t;
   }
-  ++launched_waves;
-  waves.push_back(w);
+  if (k_live) {
+    const cudaError_t q = cudaEventQuery(k_done);
+    if (q == cudaErrorNotReady) {
+      cudaGetLastError();
+      if (!stopping && t - last_busy > double(idle_ns) * 1e-9) {
+        CK(cudaMemcpyAsync(&d_q->stop, &kStop, 4, cudaMemcpyHostToDevice, up_stream));
+        stopping = true;
+      }
+      return false;
+    }
+    CK(q);
+    k_live = false;
+    stopping = false;
+  }
+  if (head_seen == tail) return false;  // no kernel runs, so head cannot have moved
+  uint32_t head = 0;
+  CK(cudaMemcpyAsync(&head, &d_q->head, 4, cudaMemcpyDeviceToHost, up_stream));
+  CK(cudaStreamSynchronize(up_stream));
+  head_seen = head;
+  if (head == tail) return false;
+  CK(cudaMemcpyAsync(&d_q->stop, &kRun, 4, cudaMemcpyHostToDevice, up_stream));
+  CK(cudaStreamSynchronize(up_stream));
+  CK(launch_serve(d_q, ctx->sm_count, P, k_stream));
+  CK(cudaEventRecord(k_done, k_stream));
+  k_live = true;
+  ++launches;
   return true;
 }
 
@@ -2330,27 +2411,12 @@ void poa_server::run() {
   try {
     for (;;) {
       bool progress = false;
-      // finished waves
-      for (size_t k = 0; k < waves.size();) {
-        const cudaError_t e = cudaEventQuery(waves[k].done);
-        if (e == cudaErrorNotReady) {
-          ++k;
-          continue;
-        }
-        CK(e);
-        Wave w = waves[k];
-        {
-          std::lock_guard<std::mutex> lk(mu);
-          waves.erase(waves.begin() + long(k));
-        }
-        finish_wave(w);
-        progress = true;
-      }
       if (finish_jobs()) progress = true;
-      if (launch_wave()) progress = true;
+      if (admit_jobs()) progress = true;
+      if (keep_kernel()) progress = true;
       std::unique_lock<std::mutex> lk(mu);
-      if (stop && pending.empty() && waves.empty()) break;
-      if (!progress) cv.wait_for(lk, std::chrono::microseconds(waves.empty() ? 2000 : 50));
+      if (stop && pending.empty() && running.empty()) break;
+      if (!progress) cv.wait_for(lk, std::chrono::microseconds(running.empty() ? 2000 : 50));
     }
   } catch (const CudaError &e) {
     std::lock_guard<std::mutex> lk(mu);
@@ -2367,7 +2433,7 @@ void poa_server::run() {
 
 extern "C" {
 
-int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_bytes, int32_t streams,
+int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_bytes, int32_t idle_ms,
                       poa_server **out) {
   if (out) *out = nullptr;
   if (!ctx || !out) return POA_ERR_INVALID;
@@ -2376,15 +2442,21 @@ int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_byte
     sv->hp = checked_params(params);
     if (sv->hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
     if (sv->hp.progressive) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
-    if (streams <= 0) streams = 64;
+    if (idle_ms > 0) sv->idle_ns = int64_t(idle_ms) * 1000000;
+    // idle DP arena pools of the context's batches go back to the budget
+    for (poa_batch *o : ctx->batches)
+      if (o->arenas) o->drop_arenas();
     const uint64_t left = ctx->budget > ctx->allocated ? ctx->budget - ctx->allocated : 0;
     if (pool_bytes == 0) pool_bytes = left > (uint64_t(512) << 20) ? left - (uint64_t(512) << 20) : 0;
     pool_bytes = pool_bytes / 256 * 256;  // the scoring tables follow the pool, 256-byte aligned
     if (pool_bytes < (uint64_t(64) << 20)) throw AlignError{POA_ERR_ALLOC, "server pool below 64 MiB"};
-    const size_t mat = sv->hp.matrix.size() * 4 + 256 + 256;
-    sv->pool_mem = (char *)ctx->dalloc(pool_bytes + mat);
+    const size_t mat = (sv->hp.matrix.size() * 4 + 255) / 256 * 256 + 256;
+    const size_t qbytes = (sizeof(ServeQueue) + 255) / 256 * 256;
+    sv->pool_mem = (char *)ctx->dalloc(pool_bytes + mat + qbytes);
     sv->ctx = ctx;
-    sv->pool_bytes = pool_bytes + mat;
+    sv->pool_bytes = pool_bytes + mat + qbytes;
+    sv->d_q = reinterpret_cast<ServeQueue *>(sv->pool_mem + pool_bytes + mat);
+    CK(cudaMemset(sv->d_q, 0, sizeof(ServeQueue)));
     int32_t *d_matrix = reinterpret_cast<int32_t *>(sv->pool_mem + pool_bytes);
     uint8_t *d_encode = reinterpret_cast<uint8_t *>(sv->pool_mem + pool_bytes + (sv->hp.matrix.size() * 4 + 255) / 256 * 256);
     CK(cudaMemcpy(d_matrix, sv->hp.matrix.data(), sv->hp.matrix.size() * 4, cudaMemcpyHostToDevice));
@@ -2392,15 +2464,11 @@ int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_byte
     CK(cudaMemcpy(d_encode, enc.data(), 256, cudaMemcpyHostToDevice));
     sv->P = poa_ctx::make_params(sv->hp, d_matrix, d_encode);
     sv->pool.init(sv->pool_mem, pool_bytes);
-    for (int k = 0; k < streams; ++k) {
-      cudaStream_t st = nullptr;
-      CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-      sv->streams.push_back(st);
-      sv->free_streams.push_back(k);
-    }
-    sv->stage.assign(size_t(streams), nullptr);
-    sv->stage_bytes.assign(size_t(streams), 0);
+    CK(cudaStreamCreateWithFlags(&sv->up_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&sv->k_stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&sv->out_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&sv->k_done, cudaEventDisableTiming));
+    sv->stages.resize(8);
     constexpr int kDoneSlots = 1 << 16;
     CK(cudaHostAlloc(reinterpret_cast<void **>(&sv->h_done), kDoneSlots * 4, cudaHostAllocMapped));
     CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&sv->d_done), sv->h_done, 0));
@@ -2474,6 +2542,9 @@ int poa_server_submit_gfa(poa_ctx *ctx, poa_server *sv, const char *gfa, int64_t
     }
     poa_server::size_job(*sj, int(sv->hp.alphabet.size()));
     sj->arena_bytes = sv->first_arena(*sj);
+    // the device image of the initial graph is built here, not by the
+    // dispatcher thread, which admits every job
+    sj->image.reset(new GraphImage(graph_image(*sj->init, sj->caps, &sj->init_rank, &sj->init_order)));
     sj->t_submit = now_s();
     std::lock_guard<std::mutex> lk(sv->mu);
     if (!sv->fatal.empty()) throw AlignError{POA_ERR_CUDA, sv->fatal};
@@ -2621,9 +2692,9 @@ int poa_server_stats_get(poa_ctx *ctx, poa_server *sv, poa_server_stats *out) {
     std::lock_guard<std::mutex> lk(sv->mu);
     out->done_jobs = sv->done_jobs;
     out->done_cells = sv->done_cells;
-    out->waves = sv->launched_waves;
+    out->waves = sv->rounds;
     out->queued = uint64_t(sv->pending.size());
-    out->running_waves = uint64_t(sv->waves.size());
+    out->kernel_launches = sv->launches;
     out->pool_bytes = sv->pool.size;
     out->pool_used = sv->pool.used;
     out->busy_s = sv->first_submit >= 0 ? sv->last_done - sv->first_submit : 0;

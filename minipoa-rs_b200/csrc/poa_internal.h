@@ -37,6 +37,26 @@ cudaError_t launch_add_node(Job *job_dev, int sigma, int base, cudaStream_t stre
 cudaError_t launch_add_edge(Job *job_dev, int from, int to, cudaStream_t stream);
 cudaError_t launch_toposort(Job *job_dev, char *arena, int64_t bytes, cudaStream_t stream);
 cudaError_t launch_reset(Job *jobs_dev, int n_jobs, int sigma, int unknown, cudaStream_t stream);
+
+// Job queue of the serving kernel, in device memory. The host publishes a
+// job by writing its descriptor's address into slot[tail % SERVE_QCAP] and
+// then raising tail (two copies in order on one stream); a warp claims the
+// entry at head with a compare-and-swap while head != tail. Bit 0 of a slot
+// marks a job to be reset to Graph::new first (descriptors are 256-byte
+// aligned). stop = 1: warps leave once the queue is empty; 2: at once.
+constexpr uint32_t SERVE_QCAP = 1u << 16;
+constexpr int SERVE_WARPS_PER_SM = 7;  // one warp's registers stay free on each SM for output kernels
+struct ServeQueue {
+  uint32_t head, tail, stop, pad;
+  unsigned long long slot[SERVE_QCAP];
+};
+// The batched kernel in serving mode (persistent): SERVE_WARPS_PER_SM warps
+// per SM claim jobs from the queue and run their reads until the host sets
+// stop; as a bound, a warp also leaves after SERVE_IDLE_LIMIT_NS without a
+// job or SERVE_MAX_POLLS empty polls.
+constexpr uint64_t SERVE_IDLE_LIMIT_NS = 10000000000ull;
+constexpr int SERVE_MAX_POLLS = 1 << 20;
+cudaError_t launch_serve(ServeQueue *q, int num_sms, const DevParams &P, cudaStream_t stream);
 int kernel_launches_per_batch();
 // Warps of the batched kernel resident on one SM (its blocks per SM x warps per block).
 int batch_resident_warps_per_sm();

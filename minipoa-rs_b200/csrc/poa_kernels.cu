@@ -20,6 +20,101 @@ __device__ __forceinline__ WarpSmem *warp_smem() {
   return reinterpret_cast<WarpSmem *>(dyn_smem) + (threadIdx.x >> 5);
 }
 
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Serving mode: lane 0 claims the next queue entry (0 when the warp is to
+// leave). An idle warp keeps polling, sleeping between empty polls (1 us,
+// doubling to 32 us), until the host sets stop, so a job published at any
+// time finds a warp; the host ends the kernel that way once the server has
+// been idle a while. Every wait is bounded: a warp also leaves after
+// SERVE_IDLE_LIMIT_NS without a job or SERVE_MAX_POLLS empty polls.
+__device__ inline unsigned long long serve_claim(ServeQueue *q) {
+  unsigned long long entry = 0;
+  if ((threadIdx.x & 31) == 0) {
+    const uint64_t t0 = globaltimer_ns();
+    unsigned sleep_ns = 1000;
+    for (int polls = 0;; ++polls) {
+      const uint32_t stop = *reinterpret_cast<volatile uint32_t *>(&q->stop);
+      if (stop >= 2) break;
+      const uint32_t h = *reinterpret_cast<volatile uint32_t *>(&q->head);
+      const uint32_t t = *reinterpret_cast<volatile uint32_t *>(&q->tail);
+      if (h != t) {
+        if (atomicCAS(&q->head, h, h + 1) == h) {
+          __threadfence();
+          entry = *reinterpret_cast<volatile unsigned long long *>(&q->slot[h & (SERVE_QCAP - 1)]);
+          break;
+        }
+        continue;
+      }
+      if (stop == 1 || polls >= SERVE_MAX_POLLS || globaltimer_ns() - t0 > SERVE_IDLE_LIMIT_NS) break;
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 32000) sleep_ns *= 2;
+    }
+  }
+  return __shfl_sync(FULL, entry, 0);
+}
+
+// Runs a job's remaining reads on the calling warp (read loop, then the
+// exact rank order), stores its status and raises its completion flag. A job
+// that outgrows its arena parks at its current read (graph untouched).
+__device__ inline void run_job(Job *J, const DevParams &P, char *arena, int64_t slot_bytes, WarpSmem *sm) {
+  const int lane = threadIdx.x & 31;
+  const int n_reads = J->n_reads;
+  char *ja = J->arena ? J->arena : arena;
+  const int64_t jb = J->arena ? J->arena_bytes : slot_bytes;
+  int32_t st = ST_OK;
+  for (int r = J->next_read; r < n_reads; ++r) {
+    st = extend_one(J, P, ja, jb, J->reads + J->read_off[r], J->read_len[r], r, sm);
+    if (st != ST_OK) break;
+  }
+  // a finished (or failed) job ends with the reference's exact rank order;
+  // a parked job keeps its order for the next pass
+  if (lane == 0) {
+    if (st == ST_OK || is_alignment_error(st)) {
+      const int32_t fs = finalize_order(J, ja, jb);
+      if (st == ST_OK) st = fs;
+    }
+    J->status = st;
+    if (J->done_flag) {
+      __threadfence_system();  // the descriptor before the flag the host polls
+      *reinterpret_cast<volatile int32_t *>(J->done_flag) = 1;
+    }
+  }
+  __syncwarp();
+}
+
+// Graph::new for one job (graph.rs:27-40: source and sink) and its counters.
+__device__ inline void reset_job(Job *J, int sigma, int unknown) {
+  J->n_nodes = 0;
+  J->n_chunks = 0;
+  J->n_edges = 0;
+  J->n_paths = 0;
+  J->path_used = 0;
+  J->n_rank = 0;
+  J->path_off[0] = 0;
+  add_node(J, sigma, unknown);
+  add_node(J, sigma, unknown);
+  J->next_read = 0;
+  J->seq_base = 0;
+  J->status = ST_OK;
+  J->err_i = J->err_j = 0;
+  J->n_items = 0;
+  J->cells = 0;
+  J->dp_bytes = 0;
+  J->pred_cells = 0;
+  J->far_preds = 0;
+  J->rows_g4 = 0;
+  J->rows_generic = 0;
+  J->coop = 0;
+  J->wave_reads = 0;
+  for (int k = 0; k < 4; ++k) J->phase[k] = 0;
+  J->order_exact = 1;
+}
+
 // Persistent batched kernel: each warp takes jobs from a size-ordered queue
 // (largest first) and runs their remaining reads. A job that outgrows the
 // warp's DP arena parks at its current read (graph untouched) for a later
@@ -34,7 +129,7 @@ __device__ __forceinline__ WarpSmem *warp_smem() {
 // the helpers join them when the giant job is done.
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     k_batch(Job *jobs, const int32_t *order, int n_jobs, int32_t *sched, int num_sms, DevParams P, char *arenas,
-            int64_t slot_bytes, int slots) {
+            int64_t slot_bytes, int slots, ServeQueue *serve) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   // the grid is rounded up to whole blocks; warps past the last slot own no
@@ -57,7 +152,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   ring_default(sm);
   __syncthreads();
   int first = -1, first_giant = 0;
-  if (active && lane == 0 && sm_ok) {
+  if (!serve && active && lane == 0 && sm_ok) {
     const int level = atomicAdd(&sm_count[smid], 1);
     if (level < SCHED_LEVELS) {
       const int64_t p0 = int64_t(level) * num_sms + atomicAdd(&level_count[level], 1);
@@ -126,40 +221,30 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   if (lane == 0 && first >= 0 && atomicExch(&claim[first], 1) != 0) first = -1;
   first = __shfl_sync(FULL, first, 0);
   for (;;) {
-    int q = first;
-    first = -1;
-    if (q < 0) {
-      if (lane == 0) {
-        do {
-          q = atomicAdd(queue, 1);
-        } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
+    Job *J = nullptr;
+    if (serve) {
+      // serving mode: the next job the host published (jobs carry their own
+      // DP arena); bit 0 of the entry asks for Graph::new first
+      const unsigned long long entry = serve_claim(serve);
+      if (entry == 0) break;
+      J = reinterpret_cast<Job *>(entry & ~1ull);
+      if ((entry & 1ull) && lane == 0) reset_job(J, P.sigma, P.unknown);
+      __syncwarp();
+    } else {
+      int q = first;
+      first = -1;
+      if (q < 0) {
+        if (lane == 0) {
+          do {
+            q = atomicAdd(queue, 1);
+          } while (q < n_jobs && atomicExch(&claim[q], 1) != 0);
+        }
+        q = __shfl_sync(FULL, q, 0);
+        if (q >= n_jobs) break;
       }
-      q = __shfl_sync(FULL, q, 0);
-      if (q >= n_jobs) break;
+      J = jobs + order[q];
     }
-    Job *J = jobs + order[q];
-    const int n_reads = J->n_reads;
-    char *ja = J->arena ? J->arena : arena;
-    const int64_t jb = J->arena ? J->arena_bytes : slot_bytes;
-    int32_t st = ST_OK;
-    for (int r = J->next_read; r < n_reads; ++r) {
-      st = extend_one(J, P, ja, jb, J->reads + J->read_off[r], J->read_len[r], r, sm);
-      if (st != ST_OK) break;
-    }
-    // a finished (or failed) job ends with the reference's exact rank order;
-    // a parked job keeps its order for the next pass
-    if (lane == 0) {
-      if (st == ST_OK || is_alignment_error(st)) {
-        const int32_t fs = finalize_order(J, ja, jb);
-        if (st == ST_OK) st = fs;
-      }
-      J->status = st;
-      if (J->done_flag) {
-        __threadfence_system();  // the descriptor before the flag the host polls
-        *reinterpret_cast<volatile int32_t *>(J->done_flag) = 1;
-      }
-    }
-    __syncwarp();
+    run_job(J, P, arena, slot_bytes, sm);
     // the giant job is done: the helpers go back to the queue
     if (sm->rv.pad[0]) coop_release(sm);
   }
@@ -308,31 +393,7 @@ __global__ void k_toposort(Job *J, char *arena, int64_t bytes) {
 // rank, no paths; the read loop restarts at read 0.
 __global__ void k_reset(Job *jobs, int n_jobs, int sigma, int unknown) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_jobs) return;
-  Job *J = jobs + j;
-  J->n_nodes = 0;
-  J->n_chunks = 0;
-  J->n_edges = 0;
-  J->n_paths = 0;
-  J->path_used = 0;
-  J->n_rank = 0;
-  J->path_off[0] = 0;
-  add_node(J, sigma, unknown);
-  add_node(J, sigma, unknown);
-  J->next_read = 0;
-  J->seq_base = 0;
-  J->status = ST_OK;
-  J->err_i = J->err_j = 0;
-  J->n_items = 0;
-  J->cells = 0;
-  J->dp_bytes = 0;
-  J->pred_cells = 0;
-  J->far_preds = 0;
-  J->rows_g4 = 0;
-  J->rows_generic = 0;
-  J->coop = 0;
-  for (int k = 0; k < 4; ++k) J->phase[k] = 0;
-  J->order_exact = 1;
+  if (j < n_jobs) reset_job(jobs + j, sigma, unknown);
 }
 
 cudaError_t prepare_batch_kernel() {
@@ -356,7 +417,16 @@ cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, 
   const cudaError_t pe = prepare_batch_kernel();
   if (pe != cudaSuccess) return pe;
   k_batch<<<blocks, wpb * 32, wpb * sizeof(WarpSmem), stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, sched,
-                                                                num_sms, P, arenas, slot_bytes, slots);
+                                                                num_sms, P, arenas, slot_bytes, slots, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_serve(ServeQueue *q, int num_sms, const DevParams &P, cudaStream_t stream) {
+  const cudaError_t pe = prepare_batch_kernel();
+  if (pe != cudaSuccess) return pe;
+  const int slots = num_sms * SERVE_WARPS_PER_SM;
+  k_batch<<<num_sms, SERVE_WARPS_PER_SM * 32, SERVE_WARPS_PER_SM * sizeof(WarpSmem), stream>>>(
+      nullptr, nullptr, 0, nullptr, num_sms, P, nullptr, 0, slots, q);
   return cudaGetLastError();
 }
 

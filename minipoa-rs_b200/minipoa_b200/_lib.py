@@ -42,7 +42,7 @@ class ServerJobInfo(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("done_jobs", ctypes.c_uint64), ("done_cells", ctypes.c_uint64), ("waves", ctypes.c_uint64),
-                ("queued", ctypes.c_uint64), ("running_waves", ctypes.c_uint64), ("pool_bytes", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64), ("pool_bytes", ctypes.c_uint64),
                 ("pool_used", ctypes.c_uint64), ("busy_s", ctypes.c_double)]
 
 
@@ -54,7 +54,7 @@ class BatchStats(ctypes.Structure):
                 ("launches", ctypes.c_int32), ("relaunches", ctypes.c_int32), ("slots", ctypes.c_int32),
                 ("reserved", ctypes.c_int32), ("kernel_ms", ctypes.c_double), ("dp_bytes", ctypes.c_uint64),
                 ("pred_cells", ctypes.c_uint64), ("far_preds", ctypes.c_uint64), ("rows_g4", ctypes.c_uint64),
-                ("rows_generic", ctypes.c_uint64), ("coop_jobs", ctypes.c_int32), ("reserved2", ctypes.c_int32),
+                ("rows_generic", ctypes.c_uint64), ("coop_jobs", ctypes.c_int32), ("wave_reads", ctypes.c_int32),
                 ("phase_cycles", ctypes.c_uint64 * 4)]
 
 

@@ -427,13 +427,13 @@ class Server:
     each finished job's graph stays resident until released. Safe to use
     from several threads (submit on one, wait on others)."""
 
-    def __init__(self, params: Params, ctx: Optional[Context] = None, pool_bytes: int = 0, streams: int = 0):
+    def __init__(self, params: Params, ctx: Optional[Context] = None, pool_bytes: int = 0, idle_ms: int = 0):
         self.ctx = ctx or default_context()
         self.L = self.ctx.L
         self.params = params
         self._c, self._keep = params.to_c()
         h = ctypes.c_void_p()
-        self.ctx.check(self.L.poa_server_create(self.ctx.h, ctypes.byref(self._c), pool_bytes, streams,
+        self.ctx.check(self.L.poa_server_create(self.ctx.h, ctypes.byref(self._c), pool_bytes, idle_ms,
                                                 ctypes.byref(h)))
         self.h = h
 

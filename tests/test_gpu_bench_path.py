@@ -9,10 +9,17 @@ ring. A small batch reaches none of these, so these tests build batches that
 do, assert from the run's counters that each path ran, and compare every
 set's output with the oracle.
 
+Static-band reads run their DP either row at a time (striped rows, the ring,
+giants with helper warps; the default) or as a row wavefront (a lane per
+row). The static-band tests run the batch once with each form forced
+(MINIPOA_DP_ROWS, read when the batch is created), once with each read's own
+choice ("auto") and once with the default.
+
 Also here: protein families with full DP (-f0, bands wider than 512 columns:
 the generic row) and an i64 set whose reads are longer than the query bytes
 kept in shared memory.
 """
+import contextlib
 import os
 
 import numpy as np
@@ -49,17 +56,37 @@ def _full_machine_sets(seed, n_giants, giant_len, giant_depth, n_small):
     return sets
 
 
+@contextlib.contextmanager
+def _dp_rows(mode):
+    """Sets the static-band DP form of batches created inside the block:
+    "rows" (row at a time), "wave" (row wavefront), "auto" (each read's
+    choice) or None (the default)."""
+    old = os.environ.get("MINIPOA_DP_ROWS")
+    if mode is None:
+        os.environ.pop("MINIPOA_DP_ROWS", None)
+    else:
+        os.environ["MINIPOA_DP_ROWS"] = mode
+    try:
+        yield
+    finally:
+        if old is None:
+            os.environ.pop("MINIPOA_DP_ROWS", None)
+        else:
+            os.environ["MINIPOA_DP_ROWS"] = old
+
+
 def _gfa_hashes_match(oracle, batch, params, sets):
     _, want = oracle.batch_run(params, sets, kernel=oracle.AUTO_AVX2, threads=THREADS, out_format=2)
     bad = [s for s in range(len(sets)) if oracle.fnv1a(batch.output(s, 2)) != want[s]]
     return bad
 
 
-@pytest.mark.parametrize("adaptive", [False, True])
-def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive):
+@pytest.mark.parametrize("adaptive,dp", [(False, "rows"), (False, "wave"), (False, "auto"), (True, None)])
+def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive, dp):
     params = Params(adaptive=adaptive)
     sets = _full_machine_sets(2024 + int(adaptive), 4, 4200, 30, 1180)
-    batch = mp.Batch(params, sets)
+    with _dp_rows(dp):
+        batch = mp.Batch(params, sets)
     st = batch.run(0)
     # one slot per resident warp of every SM in the first pass: full 8-warp
     # blocks (an adaptive giant may outgrow its arena and finish in a second
@@ -68,10 +95,15 @@ def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive):
 
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     assert st.slots == min(len(sets), sms * 8)
-    assert st.rows_g4 > 0, "no 4-stripe rows ran"
-    assert st.far_preds > 0, "no predecessor row was read back from the arena"
-    if not adaptive:
+    assert st.far_preds > 0, "no predecessor state was read back from the arena"
+    if adaptive or dp == "rows":
+        assert st.wave_reads == 0
+        assert st.rows_g4 > 0, "no 4-stripe rows ran"
+    if not adaptive and dp != "wave":
         assert st.coop_jobs >= 1, "no giant ran cooperative rows"
+    if dp == "wave":
+        # every static-band read but the giants' (their helper warps run rows)
+        assert st.wave_reads > 0, "the row wavefront did not run"
     for s in range(len(sets)):
         assert batch.status(s) is None
     # every set: GFA bytes (graph, edges in order, paths) against the oracle
@@ -122,14 +154,20 @@ def test_protein_families_full_dp_wide_rows_match_oracle(mp, oracle):
                     s.append(int(rng.integers(0, 20)))  # insertion
             fam.append(bytes(alpha[x] for x in s))
         fams.append(fam)
-    batch = mp.Batch(params, fams)
-    st = batch.run(0)
-    assert st.rows_generic > 0, "no generic (wide) rows ran"
-    for f, reads in enumerate(fams):
-        o = oracle.align_sequences(params, reads, kernel=oracle.AUTO_AVX2)
-        assert batch.graph(f).dump() == o.dump(k)
-        recs = [Sequence(name=f"read{i}", seq=x) for i, x in enumerate(reads)]
-        assert batch.output(f, 1, recs) == o.msa(params, recs)
+    for dp in ("rows", "wave"):
+        with _dp_rows(dp):
+            batch = mp.Batch(params, fams)
+        st = batch.run(0)
+        if dp == "rows":
+            assert st.rows_generic > 0, "no generic (wide) rows ran"
+        else:
+            assert st.wave_reads > 0, "the row wavefront did not run"
+        for f, reads in enumerate(fams):
+            o = oracle.align_sequences(params, reads, kernel=oracle.AUTO_AVX2)
+            assert batch.graph(f).dump() == o.dump(k)
+            recs = [Sequence(name=f"read{i}", seq=x) for i, x in enumerate(reads)]
+            assert batch.output(f, 1, recs) == o.msa(params, recs)
+        del batch
 
 
 def test_i64_reads_longer_than_shared_query_match_oracle(mp, oracle):
