@@ -61,6 +61,10 @@ def parse():
                          "--sets sets per rank (weak scaling)")
     ap.add_argument("--serve-jobs", type=int, default=1024, help="jobs of the serving loop's saturation run (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="length of the serving run at 80%% load")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="1: tune the batch's launch settings before the timed steps (0: defaults)")
+    ap.add_argument("--c4b-reads", type=int, default=3,
+                    help="reads per set of the int64 run (8 sets x 100 kbp, match 1000; 0: skip)")
     ap.add_argument("--seeded-reads", type=int, default=100,
                     help="reads of the seeded-window run (16.5 kbp ancestor, ~5%% error; 0: skip)")
     return ap.parse_args()
@@ -510,6 +514,47 @@ def c4a_bench(mp, ctx, n_fam: int = 1000, threads: int = 0):
             "parity": par}
 
 
+def c4b_bench(mp, ctx, reads_per_set: int, threads: int = 0):
+    """DNA sets whose scores overflow int32 (match score 1000, as -M1000):
+    8 sets of a 100,000 bp ancestor (seed 1005) x 20 reads at 1% error; the
+    score guard (align.rs:493-529) selects the exact int64 kernel on the GPU
+    as in the reference. Bounded: the first `reads_per_set` reads of every set
+    in one batched launch (about 0.6 G band cells per alignment); the oracle's
+    scalar int64 kernel on host threads over the first two sets with the same
+    reads; consensus bytes of those sets compared."""
+    import numpy as np
+
+    import oracle
+    from minipoa_b200 import workloads
+    from minipoa_b200.params import Params
+
+    threads = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(1005)
+    full = [workloads.read_set(rng, 100000, 20, 0.006, 0.002, 0.002) for _ in range(8)]
+    sets = [s[:reads_per_set] for s in full]
+    params = Params.from_cli_scores(match=1000)
+    o_probe = oracle.align_sequences(params, sets[0][:1])
+    i64 = not o_probe.i32_scores_safe(params, 0, 1, len(sets[0][1]))
+    b = mp.Batch(params, sets, ctx)
+    st = b.run(0)
+    out = b.output_all(0)
+    del b
+    sample = [0, 1]
+    t0 = time.perf_counter()
+    cells, hashes = oracle.batch_run(params, [sets[s] for s in sample], kernel=oracle.AUTO_AVX2,
+                                     threads=min(threads, len(sample)), out_format=0)
+    tc = time.perf_counter() - t0
+    par = consensus_parity(out, dict(zip(sample, hashes)))
+    return {"workload": f"8 sets x 100,000 bp ancestor (seed 1005), 1% error, match 1000 (-M1000): "
+                        f"the first {reads_per_set} of 20 reads per set",
+            "int64_kernel": i64, "cells": st.cells, "gpu_ms": st.device_ms,
+            "gpu_gcups": st.cells / st.device_ms / 1e6, "relaunch_passes": st.relaunches,
+            "cpu": {"gcups": cells / tc / 1e9, "cores": min(threads, len(sample)),
+                    "kind": "oracle scalar int64 kernel (the score guard's choice), one set per thread",
+                    "sample": f"sets {sample} with the same reads"},
+            "parity": par}
+
+
 def load_traffic():
     """DRAM bytes per launch of the batched kernel from the committed ncu
     summary, scaled to this run's cells (null when absent)."""
@@ -567,8 +612,18 @@ def main():
 
     ctx = mp.Context(local, mem_budget=int(args.mem_budget_gb * (1 << 30)))
     batch = mp.Batch(params, sets, ctx)
+    warm = None
     for _ in range(args.warmup):
-        batch.run(0)
+        warm = batch.run(0)
+    tuning = None
+    if args.autotune:
+        # launch settings per size bucket (warps per SM, giant threshold):
+        # every candidate runs the whole batch once; the fastest is applied
+        # and cached (the end-to-end leg's batch picks it up from the cache)
+        t = batch.autotune()
+        tuning = {"warps_per_sm": t.warps_per_sm, "giant_factor": t.giant_factor, "giant_alone": t.giant_alone,
+                  "trials": t.trials,
+                  "tuned_ms": t.device_ms, "default_ms": warm.device_ms if warm else None}
     barrier(pg)
     clocks = ClockSampler(local)
     clocks.start()
@@ -644,7 +699,12 @@ def main():
         except Exception as e:  # the throughput line above stands on its own
             serving = {"error": str(e)}
 
-    c1 = c4a = None
+    c1 = c4a = c4b = None
+    if rank == 0 and not args.no_extra and args.c4b_reads > 1:
+        try:
+            c4b = c4b_bench(mp, ctx, args.c4b_reads)
+        except Exception as e:
+            c4b = {"error": str(e)}
     if rank == 0 and not args.no_extra:
         try:
             c1 = c1_bench(mp, ctx, params)
@@ -703,7 +763,8 @@ def main():
                        "relaunch_passes": first_passes, "reads_per_s": reads / (dev_ms / 1e3),
                        "paths": {"giant_jobs_with_helpers": steps[0].coop_jobs, "rows_4_stripe": steps[0].rows_g4,
                                  "rows_generic": steps[0].rows_generic,
-                                 "pred_rows_from_arena": steps[0].far_preds}},
+                                 "pred_rows_from_arena": steps[0].far_preds},
+                       "tuning": tuning},
             "roofline": roofline,
             "roofline_int": int_roof,
             "parity": parity,
@@ -716,6 +777,7 @@ def main():
             "seeded": seeded,
             "c1_single_set": c1,
             "c4a_protein": c4a,
+            "c4b_int64": c4b,
         }
         print(json.dumps(line))
     if pg is not None:

@@ -221,6 +221,14 @@ int poa_seed_partition_windows(const poa_anchor *chain, int64_t n, int64_t tlen,
  * and poa_extend_graph run when params->seeding is set. */
 int poa_seed_anchor_windows(const poa_params *params, const uint8_t *query, int64_t qlen, const uint8_t *consensus,
                             int64_t clen, poa_anchor **out, int64_t *n_out, int32_t *tail_adaptive);
+/* guide_order (src/minimizer.rs:505-578): the order in which progressive
+ * alignment (params->progressive, -p; src/lib.rs:190-194) adds the n reads,
+ * as n read indices. Minimizer similarity from this library's sketches (see
+ * above). poa_align_sequences, poa_extend_graph (no existing records), the
+ * batched sets and the serving jobs align in this order; paths keep each
+ * read's own index. */
+int poa_seed_guide_order(const poa_params *params, int64_t n, const uint8_t *const *seqs, const int64_t *lens,
+                         int64_t **out_order);
 
 /* ---- batched independent read sets (no reference counterpart: the
  * reference runs one set per process; each set here is one extend_graph). */
@@ -290,9 +298,10 @@ int poa_graph_read_gfa(poa_ctx *ctx, const poa_params *params, const char *text,
                        char **records, int64_t *records_len);
 
 /* Autotuner (no reference counterpart). Launch settings of the batched
- * kernel: resident warps per SM and the giant threshold (a set whose
- * estimated work exceeds giant_factor per-warp shares gets three helper
- * warps; 0 = none). poa_batch_autotune runs the batch under each candidate
+ * kernel: resident warps per SM, the giant threshold (a set whose estimated
+ * work exceeds giant_factor per-warp shares gets three helper warps; 0 =
+ * none) and giant_alone (1: a giant's SM runs only the giant and its helpers
+ * until it is done). poa_batch_autotune runs the batch under each candidate
  * setting, keeps the fastest, applies it and appends it to the cache file
  * (MINIPOA_B200_TUNE_CACHE, default ~/.cache/minipoa_b200/tune.tsv) under the
  * batch's size bucket (device, log2 of set count, longest read and mean
@@ -301,7 +310,7 @@ int poa_graph_read_gfa(poa_ctx *ctx, const poa_params *params, const char *text,
  * setting (trials = runs replayed from the captured CUDA graph so far). */
 typedef struct poa_batch_tuning {
   int32_t warps_per_sm;
-  int32_t reserved;
+  int32_t giant_alone;
   double giant_factor;
   double device_ms;  /* device time of the chosen setting's run */
   int32_t trials;

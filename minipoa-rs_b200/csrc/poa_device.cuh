@@ -69,6 +69,7 @@ struct DevParams {
   int32_t relaxed_order;  // read loops may keep a spliced order between reads
   int32_t row_wave;       // static-band int32 rows: 0 one at a time, 1 wavefront where suited, 2 wavefront
   int32_t byte_prof;      // sigma <= 8 and every score fits a signed byte (dp_wave's packed profile)
+  int32_t giant_alone;    // batched runs: a giant's block keeps only the giant and its helpers
   uint64_t b, f;
   uint64_t largest;       // max(|matrix|, |O|, |E|) of i32_scores_safe
 };
@@ -100,6 +101,7 @@ struct Job {
   const int32_t *read_len;
   int32_t n_reads, next_read;
   int32_t seq_base;  // sequence id of read 0 (reads extending an imported graph follow its records)
+  const int32_t *read_id;  // when set, the sequence id of each read (reads in guide order, -p)
   // outcome
   int32_t status, err_i, err_j, n_items;
   int32_t order_exact;  // 1 when rank is the reference's LIFO toposort order
@@ -139,7 +141,7 @@ __device__ __forceinline__ uint64_t phase_clock() { return 0; }
 
 // Per-read scratch carved from the front of a warp slot's arena.
 struct Scratch {
-  int64_t *head, *tail, *support, *row_off, *wsum;
+  int64_t *head, *tail, *support, *support_b, *row_off, *wsum;
   int64_t *peak, *streak, *peak_left, *peak_right, *offset_left, *offset_right, *extra;
   int32_t *row_start, *row_len, *pred_start, *pred_cnt, *succ_start, *succ_cnt;
   int2 *pred;          // (row, weight) in incoming order; row = -1 once head is NEG
@@ -175,6 +177,7 @@ __device__ inline bool carve_scratch(char *arena, int64_t bytes, int n, int e, i
   s.head = (int64_t *)take(N * 8);
   s.tail = (int64_t *)take(N * 8);
   s.support = (int64_t *)take(N * 8);
+  s.support_b = (int64_t *)take(N * 8);
   s.row_off = (int64_t *)take(N * 8);
   s.wsum = (int64_t *)take(N * 8);
   s.peak = (int64_t *)take(N * 8);
@@ -599,7 +602,7 @@ __device__ __forceinline__ T mins(T a, T b) {
 // ring so the serial passes read their neighbours without an L2 round trip.
 constexpr int GRING = 32;
 __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int n, int64_t *ring_v,
-                                 int64_t *ring_s, Work *w) {
+                                 int64_t *ring_s, int64_t *ring_b, Work *w) {
   const int lane = threadIdx.x & 31;
   const uint64_t tg0 = phase_clock();
   int pbase = 0, sbase = 0;
@@ -709,8 +712,18 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
   // writes). Lane l holds the list start, count and first two entries of row
   // i0 + l of the current 32-row block, loaded one block ahead, and the rows
   // read them by shuffle; (head or tail, support) of the last GRING rows sit
-  // in the shared-memory ring.
-  int64_t *rv = ring_v, *rsu = ring_s;
+  // in a shared-memory ring.
+  //
+  // The forward pass (head, predecessors) and the backward pass (tail,
+  // successors) advance together, one row each per step, so the warp has two
+  // independent dependency chains to overlap. The backward pass does not
+  // depend on the forward one: the reference starts it from the sink's
+  // forward support, but every backward support is that value plus the
+  // weights along a path to the sink, so its comparisons (larger support
+  // wins a tie of weights) are the same from 0, and only head and tail leave
+  // this function. The two passes keep separate support arrays and rings
+  // (the backward ring sits in the DP ring's shared memory, unused until the
+  // DP).
   struct Lists {
     int start, cnt;
     int2 e0, e1;
@@ -725,119 +738,143 @@ __device__ inline int32_t guides(const Job *J, Scratch &s, int beg, int end, int
     }
     return L;
   };
-  // One pass (forward: predecessors, head; backward: successors, tail): per
-  // row, the first predecessor (successor) of largest weight, ties to the
-  // larger support, among those whose value is set. Rows with at most two
-  // candidates (nearly all) read both candidates' values before choosing,
-  // and the next row's list entries are taken by shuffle while this row
-  // computes.
-  auto pass = [&](bool forward, int64_t *val, const int32_t *st, const int32_t *ct, int2 *ent) {
-    const int first = forward ? 1 : n - 2;
-    const int step = forward ? 1 : -1;
-    const int count = n - 1;  // rows 1..n-1 forward, n-2..0 backward
-    auto row_of = [&](int q) { return first + step * q; };
-    Lists nxt = load(st, ct, ent, row_of(lane), lane < count);
+  struct Pass {
+    bool forward;
+    int64_t *val, *sup, *rv, *rsu;
+    const int32_t *st, *ct;
+    int2 *ent;
+    Lists cur, nxt;
+    int lb, lc;
+    int2 f0, f1;
+    int last;
+    int64_t last_v, last_s, my_v, my_s;
+    bool my_set;
+  };
+  const int count = n - 1;  // rows 1..n-1 forward, n-2..0 backward
+  auto row_of = [&](const Pass &p, int q) { return p.forward ? 1 + q : n - 2 - q; };
+  auto begin = [&](Pass &p) {
+    p.nxt = load(p.st, p.ct, p.ent, row_of(p, lane), lane < count);
     // the row computed last (row 0 forward, row n-1 backward, to begin
     // with): most rows' best candidate is that row, read from registers
-    int last = forward ? 0 : n - 1;
-    int64_t last_v = rv[last & (GRING - 1)], last_s = rsu[last & (GRING - 1)];
-    for (int q0 = 0; q0 < count; q0 += 32) {
-      const Lists cur = nxt;
-      nxt = load(st, ct, ent, row_of(q0 + 32 + lane), q0 + 32 + lane < count);
-      const int lim = min(32, count - q0);
-      // the block's results stay in the lanes (lane k: row k of the block)
-      // and are stored once at its end, so no row waits behind a store
-      int64_t my_v = 0, my_s = 0;
-      bool my_set = false;
-      int lb = __shfl_sync(FULL, cur.start, 0), lc = __shfl_sync(FULL, cur.cnt, 0);
-      int2 f0 = make_int2(__shfl_sync(FULL, cur.e0.x, 0), __shfl_sync(FULL, cur.e0.y, 0));
-      int2 f1 = make_int2(__shfl_sync(FULL, cur.e1.x, 0), __shfl_sync(FULL, cur.e1.y, 0));
-      for (int k = 0; k < lim; ++k) {
-        const int i = row_of(q0 + k);
-        const int pb = lb, pc = lc;
-        const int2 e0 = f0, e1 = f1;
-        const int kn = k + 1 < lim ? k + 1 : k;  // the next row's entries, fetched early
-        lb = __shfl_sync(FULL, cur.start, kn);
-        lc = __shfl_sync(FULL, cur.cnt, kn);
-        f0 = make_int2(__shfl_sync(FULL, cur.e0.x, kn), __shfl_sync(FULL, cur.e0.y, kn));
-        f1 = make_int2(__shfl_sync(FULL, cur.e1.x, kn), __shfl_sync(FULL, cur.e1.y, kn));
-        auto get = [&](int x, int64_t &v, int64_t &sp) {
-          if (x == last) {
-            v = last_v;
-            sp = last_s;
-            return;
-          }
-          const bool near = (forward ? i - x : x - i) < GRING;
-          v = near ? rv[x & (GRING - 1)] : val[x];
-          sp = near ? rsu[x & (GRING - 1)] : s.support[x];
-        };
-        bool have = false;
-        int bw = 0;
-        int64_t bsup = 0, bval = 0;
-        auto consider = [&](const int2 &e, int64_t v, int64_t sp, int t) {
-          if (v == NEG64) {
-            if (forward) ent[pb + t].x = -1;
-            return;
-          }
-          if (!have || e.y > bw || (e.y == bw && sp > bsup)) {
-            have = true;
-            bw = e.y;
-            bsup = sp;
-            bval = v;
-          }
-        };
-        if (pc <= 2) {
-          int64_t v0 = NEG64, s0 = 0, v1 = NEG64, s1 = 0;
-          if (pc >= 1) get(e0.x, v0, s0);
-          if (pc >= 2) get(e1.x, v1, s1);
-          if (pc >= 1) consider(e0, v0, s0, 0);
-          if (pc >= 2) consider(e1, v1, s1, 1);
-        } else {
-          for (int t = 0; t < pc; ++t) {
-            const int2 e = t == 0 ? e0 : (t == 1 ? e1 : ent[pb + t]);
-            int64_t v, sp;
-            get(e.x, v, sp);
-            consider(e, v, sp, t);
-          }
-        }
-        const int64_t vi = have ? bval + 1 : NEG64;
-        const int64_t si = have ? bsup + bw : 0;
-        if (lane == k) {
-          my_v = vi;
-          my_s = si;
-          my_set = have;
-        }
-        rv[i & (GRING - 1)] = vi;
-        rsu[i & (GRING - 1)] = si;
-        last = i;
-        last_v = vi;
-        last_s = si;
-      }
-      if (my_set) {
-        const int i = row_of(q0 + lane);
-        val[i] = my_v;
-        s.support[i] = my_s;
-      }
-      __syncwarp();  // later blocks read these rows back from memory
+    p.last = p.forward ? 0 : n - 1;
+    p.last_v = p.rv[p.last & (GRING - 1)];
+    p.last_s = p.rsu[p.last & (GRING - 1)];
+  };
+  auto block = [&](Pass &p, int q0) {
+    p.cur = p.nxt;
+    p.nxt = load(p.st, p.ct, p.ent, row_of(p, q0 + 32 + lane), q0 + 32 + lane < count);
+    p.lb = __shfl_sync(FULL, p.cur.start, 0);
+    p.lc = __shfl_sync(FULL, p.cur.cnt, 0);
+    p.f0 = make_int2(__shfl_sync(FULL, p.cur.e0.x, 0), __shfl_sync(FULL, p.cur.e0.y, 0));
+    p.f1 = make_int2(__shfl_sync(FULL, p.cur.e1.x, 0), __shfl_sync(FULL, p.cur.e1.y, 0));
+    // the block's results stay in the lanes (lane k: row k of the block)
+    // and are stored once at its end
+    p.my_v = p.my_s = 0;
+    p.my_set = false;
+  };
+  auto block_end = [&](Pass &p, int q0) {
+    if (p.my_set) {
+      const int i = row_of(p, q0 + lane);
+      p.val[i] = p.my_v;
+      p.sup[i] = p.my_s;
     }
   };
-  // forward: head along the heaviest (then most supported) predecessor
+  // One row of a pass: the first predecessor (successor) of largest weight,
+  // ties to the larger support, among those whose value is set. Rows with at
+  // most two candidates (nearly all) read both candidates' values before
+  // choosing, and the next row's list entries are taken by shuffle while
+  // this row computes.
+  auto step = [&](Pass &p, int q0, int k, int lim) {
+    const bool forward = p.forward;
+    const int i = row_of(p, q0 + k);
+    const int pb = p.lb, pc = p.lc;
+    const int2 e0 = p.f0, e1 = p.f1;
+    const int kn = k + 1 < lim ? k + 1 : k;  // the next row's entries, fetched early
+    p.lb = __shfl_sync(FULL, p.cur.start, kn);
+    p.lc = __shfl_sync(FULL, p.cur.cnt, kn);
+    p.f0 = make_int2(__shfl_sync(FULL, p.cur.e0.x, kn), __shfl_sync(FULL, p.cur.e0.y, kn));
+    p.f1 = make_int2(__shfl_sync(FULL, p.cur.e1.x, kn), __shfl_sync(FULL, p.cur.e1.y, kn));
+    auto get = [&](int x, int64_t &v, int64_t &sp) {
+      if (x == p.last) {
+        v = p.last_v;
+        sp = p.last_s;
+        return;
+      }
+      const bool near = (forward ? i - x : x - i) < GRING;
+      v = near ? p.rv[x & (GRING - 1)] : p.val[x];
+      sp = near ? p.rsu[x & (GRING - 1)] : p.sup[x];
+    };
+    bool have = false;
+    int bw = 0;
+    int64_t bsup = 0, bval = 0;
+    auto consider = [&](const int2 &e, int64_t v, int64_t sp, int t) {
+      if (v == NEG64) {
+        if (forward) p.ent[pb + t].x = -1;
+        return;
+      }
+      if (!have || e.y > bw || (e.y == bw && sp > bsup)) {
+        have = true;
+        bw = e.y;
+        bsup = sp;
+        bval = v;
+      }
+    };
+    if (pc <= 2) {
+      int64_t v0 = NEG64, s0 = 0, v1 = NEG64, s1 = 0;
+      if (pc >= 1) get(e0.x, v0, s0);
+      if (pc >= 2) get(e1.x, v1, s1);
+      if (pc >= 1) consider(e0, v0, s0, 0);
+      if (pc >= 2) consider(e1, v1, s1, 1);
+    } else {
+      for (int t = 0; t < pc; ++t) {
+        const int2 e = t == 0 ? e0 : (t == 1 ? e1 : p.ent[pb + t]);
+        int64_t v, sp;
+        get(e.x, v, sp);
+        consider(e, v, sp, t);
+      }
+    }
+    const int64_t vi = have ? bval + 1 : NEG64;
+    const int64_t si = have ? bsup + bw : 0;
+    if (lane == k) {
+      p.my_v = vi;
+      p.my_s = si;
+      p.my_set = have;
+    }
+    p.rv[i & (GRING - 1)] = vi;
+    p.rsu[i & (GRING - 1)] = si;
+    p.last = i;
+    p.last_v = vi;
+    p.last_s = si;
+  };
+  Pass F{true, s.head, s.support, ring_v, ring_s, s.pred_start, s.pred_cnt, s.pred};
+  Pass B{false, s.tail, s.support_b, ring_b, ring_b + GRING, s.succ_start, s.succ_cnt, s.succ};
   const uint64_t tg1 = phase_clock();
+  // forward from the source (head 0), backward from the sink (tail 1)
   s.head[0] = 0;
-  rv[0] = 0;
-  rsu[0] = 0;
-  pass(true, s.head, s.pred_start, s.pred_cnt, s.pred);
-  const uint64_t tg2 = phase_clock();
-  // backward: tail along the heaviest (then most supported) successor; the
-  // support array continues from the forward pass
+  ring_v[0] = 0;
+  ring_s[0] = 0;
   s.tail[n - 1] = 1;
-  rv[(n - 1) & (GRING - 1)] = 1;  // rsu keeps the forward support of the last row
-  pass(false, s.tail, s.succ_start, s.succ_cnt, s.succ);
+  s.support_b[n - 1] = 0;
+  ring_b[(n - 1) & (GRING - 1)] = 1;
+  ring_b[GRING + ((n - 1) & (GRING - 1))] = 0;
+  begin(F);
+  begin(B);
+  for (int q0 = 0; q0 < count; q0 += 32) {
+    block(F, q0);
+    block(B, q0);
+    const int lim = min(32, count - q0);
+    for (int k = 0; k < lim; ++k) {
+      step(F, q0, k, lim);
+      step(B, q0, k, lim);
+    }
+    block_end(F, q0);
+    block_end(B, q0);
+    __syncwarp();  // later blocks read these rows back from memory
+  }
   __syncwarp();
   (void)w;
   (void)tg0;
   (void)tg1;
-  (void)tg2;
   return s.head[n - 1] == NEG64 ? ST_NO_PATH : ST_OK;
 }
 
@@ -2156,7 +2193,8 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
   const S s00 = S(P.matrix[P.unknown * P.sigma + P.unknown]);
   __syncwarp();
   const uint64_t t_g0 = phase_clock();
-  int32_t st = guides(J, s, beg, end, n, sm ? sm->gring_v : nullptr, sm ? sm->gring_s : nullptr, cells);
+  // the backward guide pass's ring borrows the DP ring's shared memory
+  int32_t st = guides(J, s, beg, end, n, sm->gring_v, sm->gring_s, reinterpret_cast<int64_t *>(sm->ring_d), cells);
   const uint64_t t_g1 = phase_clock();
   cells->phase[0] += t_g1 - t_g0;
   if (st != ST_OK) return st;
@@ -2807,8 +2845,9 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   const uint64_t t_u0 = phase_clock();
   const int n_old = J->n_nodes;
   int32_t *mark = s.dp_bytes >= int64_t(n_old) * 4 ? reinterpret_cast<int32_t *>(s.dp) : nullptr;
-  if (!add_path_warp(J, P, J->seq_base + r, s.items, n_items, &st, mark)) {
-    if (lane == 0) st = add_path(J, P, J->seq_base + r, s.items, n_items);
+  const int sid = J->read_id ? J->read_id[r] : J->seq_base + r;
+  if (!add_path_warp(J, P, sid, s.items, n_items, &st, mark)) {
+    if (lane == 0) st = add_path(J, P, sid, s.items, n_items);
     st = __shfl_sync(FULL, st, 0);
   }
   __syncwarp();

@@ -582,11 +582,22 @@ HostParams checked_params(const poa_params *p) {
 }
 
 // Runs the single-graph read loop reads[r0..r1) with arena growth on demand.
-void extend_range(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::vector<const uint8_t *> &seqs,
-                  const std::vector<int64_t> &lens, int64_t r0) {
-  if (hp.progressive && r0 == 0) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
-  const int64_t n = int64_t(seqs.size());
+void extend_range(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::vector<const uint8_t *> &seqs_in,
+                  const std::vector<int64_t> &lens_in, int64_t r0) {
+  const int64_t n = int64_t(seqs_in.size());
   if (r0 >= n) return;
+  // progressive (-p, src/lib.rs:190-194): the reads go in guide order and
+  // keep their own sequence ids
+  std::vector<int64_t> order;
+  if (hp.progressive && r0 == 0) order = guide_order(hp, seqs_in, lens_in);
+  const bool ordered = !order.empty();
+  std::vector<const uint8_t *> seqs(seqs_in);
+  std::vector<int64_t> lens(lens_in);
+  if (ordered)
+    for (int64_t k = 0; k < n; ++k) {
+      seqs[size_t(k)] = seqs_in[size_t(order[size_t(k)])];
+      lens[size_t(k)] = lens_in[size_t(order[size_t(k)])];
+    }
   int64_t total = 0, maxlen = 0;
   for (int64_t r = r0; r < n; ++r) {
     if (lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
@@ -595,29 +606,33 @@ void extend_range(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::v
   }
   g->reserve(total + 2 * (n - r0), 2 * (total + 3 * (n - r0)), total + (n - r0), n - r0);
   DevParams P = ctx->params(hp);
-  // reads, offsets and lengths in one upload
-  const size_t off_bytes = size_t(n) * 8, len_bytes = size_t(n) * 4;
-  const size_t need = off_bytes + len_bytes + size_t(std::max<int64_t>(total, 1)) + 64;
+  // reads, offsets, lengths and sequence ids in one upload
+  const size_t off_bytes = size_t(n) * 8, len_bytes = size_t(n) * 4, id_bytes = size_t(n) * 4;
+  const size_t need = off_bytes + len_bytes + id_bytes + size_t(std::max<int64_t>(total, 1)) + 64;
   ctx->ensure_qbuf(need);
   std::vector<uint8_t> host(need);
   int64_t *off = (int64_t *)host.data();
   int32_t *ln = (int32_t *)(host.data() + off_bytes);
-  uint8_t *rd = host.data() + off_bytes + len_bytes;
+  int32_t *ids = (int32_t *)(host.data() + off_bytes + len_bytes);
+  uint8_t *rd = host.data() + off_bytes + len_bytes + id_bytes;
   int64_t at = 0;
   for (int64_t r = 0; r < n; ++r) {
     off[r] = at;
     ln[r] = int32_t(r >= r0 ? lens[r] : 0);
+    ids[r] = int32_t(ordered ? order[size_t(r)] : r);
     if (r >= r0 && lens[r] > 0) std::memcpy(rd + at, seqs[r], size_t(lens[r]));
     if (r >= r0) at += lens[r];
   }
   CK(cudaMemcpyAsync(ctx->qbuf, host.data(), need, cudaMemcpyHostToDevice, ctx->stream));
   const int64_t *d_off = (const int64_t *)ctx->qbuf;
   const int32_t *d_len = (const int32_t *)(ctx->qbuf + off_bytes);
-  const uint8_t *d_rd = ctx->qbuf + off_bytes + len_bytes;
+  const int32_t *d_ids = (const int32_t *)(ctx->qbuf + off_bytes + len_bytes);
+  const uint8_t *d_rd = ctx->qbuf + off_bytes + len_bytes + id_bytes;
   // the device advances next_read after each completed read
   g->sync();
   g->h.next_read = int32_t(r0);
   g->h.status = ST_OK;
+  g->h.read_id = ordered ? d_ids : nullptr;
   g->upload();
   // initial arena: scratch + a static-band estimate, grown on ARENA_FULL
   int64_t arena = std::max<int64_t>(int64_t(64) << 20, ctx->arena_bytes);
@@ -822,8 +837,10 @@ std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, p
 // the device after the last read.
 void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::vector<const uint8_t *> &seqs,
                    const std::vector<int64_t> &lens, int64_t r0) {
-  if (hp.progressive && r0 == 0) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
   const int64_t n = int64_t(seqs.size());
+  // progressive (-p, src/lib.rs:190-194): reads in guide order, own ids
+  std::vector<int64_t> order;
+  if (hp.progressive && r0 == 0) order = guide_order(hp, seqs, lens);
   int64_t total = 0;
   for (int64_t r = r0; r < n; ++r) {
     if (lens[size_t(r)] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
@@ -832,7 +849,8 @@ void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::
   g->reserve(total + 2 * (n - r0), 2 * (total + 3 * (n - r0)), total + (n - r0), n - r0);
   const DevParams P = ctx->params(hp);
   bool stale = false;
-  for (int64_t r = r0; r < n; ++r) {
+  for (int64_t k = r0; k < n; ++k) {
+    const int64_t r = order.empty() ? k : order[size_t(k)];
     auto path = seeded_align(ctx, hp, g, seqs[size_t(r)], lens[size_t(r)], stale);
     std::vector<int4> it(path.size());
     for (size_t k = 0; k < path.size(); ++k)
@@ -893,11 +911,13 @@ struct poa_batch {
   uint64_t h2d_bytes = 0, d2h_bytes = 0;
   std::vector<double> est;     // estimated work per set (size order, giants, tuning bucket)
   double giant_factor = 1.5;   // giant: estimated work above this many per-warp shares
+  int giant_alone = 0;         // a giant's SM runs only its team (see DevParams::giant_alone)
   std::string tune_key;        // autotuner cache key of the batch's size bucket
   // the first pass of a batched run (reset, queue set-up, persistent kernel)
   // captured once as a CUDA graph and replayed while its launch shape holds
   cudaGraphExec_t gexec = nullptr;
   int64_t g_slots = -1, g_slot_bytes = -1;
+  int g_alone = -1;
   int graph_launches = 0;
 
   // d_order holds two orders: the running pass's, and at base_order() the
@@ -1406,7 +1426,7 @@ int poa_graph_export(poa_ctx *ctx, poa_graph *graph, int64_t *fields, int64_t *r
 // ---- batch autotuner cache
 
 // Tuned launch settings per device and batch size bucket: one line
-// "key<TAB>warps_per_sm<TAB>giant_factor" per bucket in the file named by
+// "key<TAB>warps_per_sm<TAB>giant_factor<TAB>giant_alone" per bucket in the file named by
 // MINIPOA_B200_TUNE_CACHE (default ~/.cache/minipoa_b200/tune.tsv).
 std::string tune_path() {
   if (const char *p = std::getenv("MINIPOA_B200_TUNE_CACHE")) return p;
@@ -1437,7 +1457,7 @@ std::string tune_key(poa_ctx *ctx, int64_t n_sets, const int64_t *set_off, const
 
 std::mutex g_tune_mu;
 
-bool tune_lookup(const std::string &key, int *warps_per_sm, double *giant_factor) {
+bool tune_lookup(const std::string &key, int *warps_per_sm, double *giant_factor, int *giant_alone) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   std::ifstream f(tune_path());
   std::string line;
@@ -1445,14 +1465,16 @@ bool tune_lookup(const std::string &key, int *warps_per_sm, double *giant_factor
   while (std::getline(f, line)) {
     const size_t a = line.find('\t'), b = a == std::string::npos ? a : line.find('\t', a + 1);
     if (b == std::string::npos || line.substr(0, a) != key) continue;
+    const size_t c = line.find('\t', b + 1);
     *warps_per_sm = std::atoi(line.substr(a + 1, b - a - 1).c_str());
-    *giant_factor = std::atof(line.substr(b + 1).c_str());
+    *giant_factor = std::atof(line.substr(b + 1, c == std::string::npos ? std::string::npos : c - b - 1).c_str());
+    *giant_alone = c == std::string::npos ? 0 : std::atoi(line.substr(c + 1).c_str());
     found = true;  // the last entry for a key wins
   }
   return found;
 }
 
-void tune_store(const std::string &key, int warps_per_sm, double giant_factor) {
+void tune_store(const std::string &key, int warps_per_sm, double giant_factor, int giant_alone) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   const std::string path = tune_path();
   const size_t slash = path.rfind('/');
@@ -1465,7 +1487,7 @@ void tune_store(const std::string &key, int warps_per_sm, double giant_factor) {
       }
   }
   std::ofstream f(path, std::ios::app);
-  f << key << '\t' << warps_per_sm << '\t' << giant_factor << '\n';
+  f << key << '\t' << warps_per_sm << '\t' << giant_factor << '\t' << giant_alone << '\n';
 }
 
 int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, const int64_t *set_off,
@@ -1474,7 +1496,6 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
   return api(ctx, [&] {
     HostParams hp = checked_params(params);
     if (hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
-    if (hp.progressive) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
     auto b = std::make_unique<poa_batch>();
     b->ctx = ctx;
     b->hp = hp;
@@ -1490,23 +1511,44 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
       if (lens[r] < 0 || lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
       total += lens[r];
     }
-    const size_t off_bytes = size_t(n_reads) * 8 + 8, len_bytes = size_t(n_reads) * 4 + 4;
-    b->reads_bytes = off_bytes + len_bytes + size_t(total) + 64;
+    // progressive (-p, src/lib.rs:190-194): each set's reads are uploaded in
+    // its guide order, with their own sequence ids beside them
+    std::vector<int64_t> src(static_cast<size_t>(n_reads));
+    std::vector<int32_t> rid(static_cast<size_t>(n_reads));
+    for (int64_t st = 0; st < n_sets; ++st) {
+      const int64_t a = set_off[st], k = set_off[st + 1] - a;
+      std::vector<int64_t> order;
+      if (hp.progressive)
+        order = guide_order(hp, std::vector<const uint8_t *>(seqs + a, seqs + a + k),
+                            std::vector<int64_t>(lens + a, lens + a + k));
+      for (int64_t q = 0; q < k; ++q) {
+        const int64_t o = order.empty() ? q : order[size_t(q)];
+        src[size_t(a + q)] = a + o;
+        rid[size_t(a + q)] = int32_t(o);
+      }
+    }
+    const size_t off_bytes = size_t(n_reads) * 8 + 8, len_bytes = size_t(n_reads) * 4 + 4,
+                 id_bytes = size_t(n_reads) * 4 + 4;
+    b->reads_bytes = off_bytes + len_bytes + id_bytes + size_t(total) + 64;
     char *rb = (char *)ctx->dalloc(b->reads_bytes);
     b->d_read_off = (int64_t *)rb;
     b->d_read_len = (int32_t *)(rb + off_bytes);
-    b->d_reads = (uint8_t *)(rb + off_bytes + len_bytes);
+    int32_t *d_read_id = (int32_t *)(rb + off_bytes + len_bytes);
+    b->d_reads = (uint8_t *)(rb + off_bytes + len_bytes + id_bytes);
     {
       std::vector<char> host(b->reads_bytes);
       int64_t *off = (int64_t *)host.data();
       int32_t *ln = (int32_t *)(host.data() + off_bytes);
-      char *rd = host.data() + off_bytes + len_bytes;
+      int32_t *ids = (int32_t *)(host.data() + off_bytes + len_bytes);
+      char *rd = host.data() + off_bytes + len_bytes + id_bytes;
       int64_t at = 0;
       for (int64_t r = 0; r < n_reads; ++r) {
+        const int64_t o = src[size_t(r)];
         off[r] = at;
-        ln[r] = int32_t(lens[r]);
-        if (lens[r]) std::memcpy(rd + at, seqs[r], size_t(lens[r]));
-        at += lens[r];
+        ln[r] = int32_t(lens[o]);
+        ids[r] = rid[size_t(r)];
+        if (lens[o]) std::memcpy(rd + at, seqs[o], size_t(lens[o]));
+        at += lens[o];
       }
       CK(cudaMemcpyAsync(rb, host.data(), b->reads_bytes, cudaMemcpyHostToDevice, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
@@ -1545,6 +1587,7 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
       J.reads = b->d_reads;
       J.read_off = b->d_read_off + set_off[s];
       J.read_len = b->d_read_len + set_off[s];
+      J.read_id = hp.progressive ? d_read_id + set_off[s] : nullptr;
       J.n_reads = int32_t(set_off[s + 1] - set_off[s]);
     }
     b->d_jobs = (Job *)ctx->dalloc(b->jobs.size() * sizeof(Job) + 16);
@@ -1567,7 +1610,7 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return est[a] > est[c]; });
     b->est = est;
     b->tune_key = tune_key(ctx, n_sets, set_off, lens);
-    tune_lookup(b->tune_key, &b->warps_per_sm, &b->giant_factor);
+    tune_lookup(b->tune_key, &b->warps_per_sm, &b->giant_factor, &b->giant_alone);
     b->mark_giants();
     b->upload_jobs();
     b->d_order = (int32_t *)ctx->dalloc(b->order_bytes());
@@ -1585,19 +1628,22 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
 
 int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
   return api(ctx, [&] {
-    // candidate launch settings: resident warps per SM and the giant
-    // threshold (0: no giant gets helper warps)
-    const int wps_c[] = {8, 8, 8, 6, 4};
-    const double gf_c[] = {1.5, 3.0, 0.0, 1.5, 1.5};
-    const int keep_w = b->warps_per_sm;
-    const double keep_g = b->giant_factor;
+    // candidate launch settings: resident warps per SM, the giant threshold
+    // (0: no giant gets helper warps) and whether a giant's SM runs its team
+    // alone; the first is the default
+    struct Cand {
+      int wps;
+      double gf;
+      int alone;
+    };
+    const Cand cand[] = {{8, 1.5, 0}, {8, 1.5, 1}, {8, 3.0, 1}, {6, 1.5, 0}, {4, 1.5, 0}, {4, 3.0, 0}, {8, 0.0, 0}};
     double best_ms = 0;
-    int best_w = keep_w;
-    double best_g = keep_g;
+    Cand best{b->warps_per_sm, b->giant_factor, b->giant_alone};
     int tried = 0;
-    for (int k = 0; k < 5; ++k) {
-      b->warps_per_sm = wps_c[k];
-      b->giant_factor = gf_c[k];
+    for (const Cand &c : cand) {
+      b->warps_per_sm = c.wps;
+      b->giant_factor = c.gf;
+      b->giant_alone = c.alone;
       b->mark_giants();
       b->upload_jobs();
       poa_batch_stats st{};
@@ -1606,19 +1652,19 @@ int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
       ++tried;
       if (tried == 1 || st.device_ms < best_ms) {
         best_ms = st.device_ms;
-        best_w = wps_c[k];
-        best_g = gf_c[k];
+        best = c;
       }
     }
-    b->warps_per_sm = best_w;
-    b->giant_factor = best_g;
+    b->warps_per_sm = best.wps;
+    b->giant_factor = best.gf;
+    b->giant_alone = best.alone;
     b->mark_giants();
     b->upload_jobs();
-    tune_store(b->tune_key, best_w, best_g);
+    tune_store(b->tune_key, best.wps, best.gf, best.alone);
     if (out) {
-      out->warps_per_sm = best_w;
-      out->reserved = 0;
-      out->giant_factor = best_g;
+      out->warps_per_sm = best.wps;
+      out->giant_alone = best.alone;
+      out->giant_factor = best.gf;
       out->device_ms = best_ms;
       out->trials = tried;
     }
@@ -1628,7 +1674,7 @@ int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
 int poa_batch_tuning_get(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
   return api(ctx, [&] {
     out->warps_per_sm = b->warps_per_sm > 0 ? b->warps_per_sm : batch_resident_warps_per_sm();
-    out->reserved = 0;
+    out->giant_alone = b->giant_alone;
     out->giant_factor = b->giant_factor;
     out->device_ms = 0;
     out->trials = b->graph_launches;
@@ -1678,7 +1724,8 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
           slots_first = int(slots);
           // the first pass as one CUDA graph (reset of every graph, queue
           // set-up, the persistent kernel), captured once per launch shape
-          if (!b->gexec || b->g_slots != slots || b->g_slot_bytes != slot_bytes) {
+          b->P.giant_alone = b->giant_alone;
+          if (!b->gexec || b->g_slots != slots || b->g_slot_bytes != slot_bytes || b->g_alone != b->giant_alone) {
             if (b->gexec) cudaGraphExecDestroy(b->gexec);
             b->gexec = nullptr;
             CK(prepare_batch_kernel());
@@ -1700,6 +1747,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
             CK(ce);
             b->g_slots = slots;
             b->g_slot_bytes = slot_bytes;
+            b->g_alone = b->giant_alone;
           }
           // timing events stay outside the graph: an event recorded during
           // capture becomes a dependency marker, not a timestamp
@@ -1992,8 +2040,9 @@ struct PoolAlloc {
 
 struct ServerJob {
   int64_t id = 0;
-  std::vector<uint8_t> bytes;  // the reads, back to back
+  std::vector<uint8_t> bytes;  // the reads, back to back (in guide order with -p)
   std::vector<int64_t> lens;
+  std::vector<int32_t> ids;    // with -p, the sequence id of each read as stored
   // an initial graph to extend (GFA jobs): built and ranked on the host at
   // submission, copied into the job's storage at admission; the job's reads
   // get sequence ids after its `existing` path records
@@ -2114,7 +2163,7 @@ struct poa_server {
     sj.caps = c;
     Job J{};
     sj.storage_bytes = layout(c, nullptr, &J) + 256;
-    sj.reads_bytes = uint64_t(k) * 12 + uint64_t(sum) + 64;
+    sj.reads_bytes = uint64_t(k) * 16 + uint64_t(sum) + 64;  // offsets, lengths, ids, bytes
   }
   // First DP arena of a job: band cells of its widest read over an estimate of
   // the rows the graph grows to, plus per-row scratch; a job that needs more
@@ -2314,7 +2363,8 @@ bool poa_server::admit_jobs() {
       const int64_t n = int64_t(sj.lens.size());
       J.read_off = reinterpret_cast<int64_t *>(sj.reads);
       J.read_len = reinterpret_cast<int32_t *>(sj.reads + n * 8);
-      J.reads = reinterpret_cast<uint8_t *>(sj.reads + n * 12);
+      J.read_id = sj.ids.empty() ? nullptr : reinterpret_cast<int32_t *>(sj.reads + n * 12);
+      J.reads = reinterpret_cast<uint8_t *>(sj.reads + n * 16);
       J.n_reads = int32_t(n);
       char *host = staging + staged;
       staged += PoolAlloc::round(sj.reads_bytes);
@@ -2323,9 +2373,10 @@ bool poa_server::admit_jobs() {
       for (int64_t r = 0; r < n; ++r) {
         reinterpret_cast<int64_t *>(host)[r] = at;
         reinterpret_cast<int32_t *>(host + n * 8)[r] = int32_t(sj.lens[size_t(r)]);
+        reinterpret_cast<int32_t *>(host + n * 12)[r] = sj.ids.empty() ? int32_t(r) : sj.ids[size_t(r)];
         at += sj.lens[size_t(r)];
       }
-      if (!sj.bytes.empty()) std::memcpy(host + n * 12, sj.bytes.data(), sj.bytes.size());
+      if (!sj.bytes.empty()) std::memcpy(host + n * 16, sj.bytes.data(), sj.bytes.size());
       CK(cudaMemcpyAsync(sj.reads, host, sj.reads_bytes, cudaMemcpyHostToDevice, up_stream));
       sj.J = J;
       sj.t_start = t;
@@ -2441,7 +2492,6 @@ int poa_server_create(poa_ctx *ctx, const poa_params *params, uint64_t pool_byte
   const int rc = api(ctx, [&] {
     sv->hp = checked_params(params);
     if (sv->hp.seeding) throw AlignError{POA_ERR_UNSUPPORTED, "seeded windows (-S) are not available in this build"};
-    if (sv->hp.progressive) throw AlignError{POA_ERR_UNSUPPORTED, "progressive guide order (-p) is not available in this build"};
     if (idle_ms > 0) sv->idle_ns = int64_t(idle_ms) * 1000000;
     // idle DP arena pools of the context's batches go back to the budget
     for (poa_batch *o : ctx->batches)
@@ -2492,10 +2542,19 @@ int poa_server_submit(poa_ctx *ctx, poa_server *sv, int64_t n_seqs, const uint8_
       if (lens[r] < 0 || lens[r] > INT32_MAX / 4) throw AlignError{POA_ERR_INVALID, "sequence is too long"};
       total += lens[r];
     }
+    // progressive (-p, src/lib.rs:190-194): the reads are stored in guide
+    // order with their own sequence ids
+    std::vector<int64_t> order;
+    if (sv->hp.progressive)
+      order = guide_order(sv->hp, std::vector<const uint8_t *>(seqs, seqs + n_seqs),
+                          std::vector<int64_t>(lens, lens + n_seqs));
     sj->bytes.resize(size_t(total));
-    sj->lens.assign(lens, lens + n_seqs);
+    sj->lens.resize(size_t(n_seqs));
     int64_t at = 0;
-    for (int64_t r = 0; r < n_seqs; ++r) {
+    for (int64_t q = 0; q < n_seqs; ++q) {
+      const int64_t r = order.empty() ? q : order[size_t(q)];
+      sj->lens[size_t(q)] = lens[r];
+      if (!order.empty()) sj->ids.push_back(int32_t(r));
       if (lens[r]) std::memcpy(sj->bytes.data() + at, seqs[r], size_t(lens[r]));
       at += lens[r];
     }

@@ -205,6 +205,10 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   } else if (!active) {
     return;
   }
+  // giant_alone: the giant's SM keeps only its team (the giant and its
+  // helpers, which take other jobs once it is done); the block's other warps
+  // leave, and their first positions, left unclaimed, go to the shared queue
+  if (P.giant_alone && coop_block && me != lead && !(me >= h0 && me < h0 + 3)) return;
   first = __shfl_sync(FULL, first, 0);
   first_giant = __shfl_sync(FULL, first_giant, 0);
   if (first_giant && coop_block) {

@@ -108,12 +108,12 @@ __global__ void k_align_noalloc(Job *J, DevParams P, char *arena, int64_t bytes,
 // graph of n rows and e edges and a query of qlen bases.
 int64_t scratch_floor(int64_t n, int64_t e, int64_t qlen) {
   const int64_t padded = (qlen + 2) / 8 * 8 + 8;
-  // per row: 12 int64 arrays, 8 int32 arrays, an int4 plan and an 80-byte
+  // per row: 13 int64 arrays, 8 int32 arrays, an int4 plan and an 80-byte
   // wavefront record; per edge entry:
   // pred, succ, pmeta, pmeta_off, two traceback descriptors, pent; the query
   // as int32 and as bytes; the result items; 128-byte alignment of 36 arrays
-  return n * (12 * 8 + 8 * 4 + 16 + 80) + (e + 1) * (8 + 8 + 16 + 8 + 32 + 16) + (padded + 32) * 5 +
-         (qlen + 4) * 16 + 36 * 128;
+  return n * (13 * 8 + 8 * 4 + 16 + 80) + (e + 1) * (8 + 8 + 16 + 8 + 32 + 16) + (padded + 32) * 5 +
+         (qlen + 4) * 16 + 37 * 128;
 }
 
 }  // namespace

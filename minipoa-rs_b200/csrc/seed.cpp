@@ -390,6 +390,81 @@ std::pair<std::vector<Anchor>, bool> anchor_windows(const HostParams &p, const u
   return partition_windows(ch, clen, qlen, int64_t(p.win_band), max_win);
 }
 
+// src/minimizer.rs:505-578. Reads are compared by the minimizers they share:
+// a minimizer value carried by more than mm_filter_ratio x n reads is
+// dropped; per pair, the shared count is the sum over values of the smaller
+// multiplicity, and the similarity is shared / (total_a + total_b - shared)
+// weighted by 0.51 len_a / max_len + 0.49 len_b / max_len (so it is
+// directional). The most similar ordered pair starts the order; each next
+// read is the unused one of largest summed similarity to the reads already
+// ordered (ties to the smaller index). Minimizers are this library's own
+// (sketch above), so the order is the reference's only where the sketches
+// agree.
+std::vector<int64_t> guide_order(const HostParams &p, const std::vector<const uint8_t *> &seqs,
+                                 const std::vector<int64_t> &lens) {
+  const int64_t n = int64_t(seqs.size());
+  std::vector<int64_t> input(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) input[size_t(i)] = i;
+  if (!p.progressive || n < 2 || p.alphabet.size() > 5) return input;
+  // value -> (read -> multiplicity), both in ascending order
+  std::map<uint64_t, std::map<int64_t, int64_t>> groups;
+  for (int64_t r = 0; r < n; ++r)
+    for (const Minimizer &mm : sketch(seqs[size_t(r)], lens[size_t(r)], int64_t(p.k), int64_t(p.w)))
+      ++groups[mm.value][r];
+  if (groups.empty()) return input;
+  std::vector<int64_t> total(static_cast<size_t>(n), 0), shared(static_cast<size_t>(n * n), 0);
+  for (const auto &g : groups) {
+    const auto &counts = g.second;
+    if (double(counts.size()) > double(n) * p.mm_filter_ratio) continue;
+    for (auto ia = counts.begin(); ia != counts.end(); ++ia) {
+      const int64_t a = ia->first, ca = ia->second;
+      total[size_t(a)] += ca;
+      for (auto ib = counts.begin(); ib != ia; ++ib) {
+        const int64_t b = ib->first, m = std::min(ca, ib->second);
+        shared[size_t(a * n + b)] += m;
+        shared[size_t(b * n + a)] += m;
+      }
+    }
+  }
+  int64_t mx = 1;
+  for (int64_t l : lens) mx = std::max(mx, l);
+  const double max_len = double(mx);
+  std::vector<double> sim(static_cast<size_t>(n * n), 0.0);
+  double best = -1.0;
+  int64_t bi = 0, bj = 1;
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t j = 0; j < n; ++j) {
+      if (i == j) continue;
+      const int64_t common = shared[size_t(i * n + j)];
+      const int64_t uni = total[size_t(i)] + total[size_t(j)] - common;
+      const double jac = uni == 0 ? 0.0
+                                  : double(common) / double(uni) *
+                                        (0.51 * double(lens[size_t(i)]) / max_len +
+                                         0.49 * double(lens[size_t(j)]) / max_len);
+      sim[size_t(i * n + j)] = jac;
+      if (jac > best) {
+        best = jac;
+        bi = i;
+        bj = j;
+      }
+    }
+  std::vector<int64_t> order{bi, bj};
+  std::vector<char> used(static_cast<size_t>(n), 0);
+  used[size_t(bi)] = used[size_t(bj)] = 1;
+  std::vector<double> sums(static_cast<size_t>(n));
+  for (int64_t v = 0; v < n; ++v) sums[size_t(v)] = sim[size_t(bi * n + v)] + sim[size_t(bj * n + v)];
+  while (int64_t(order.size()) < n) {
+    int64_t next = -1;
+    for (int64_t v = 0; v < n; ++v)
+      if (!used[size_t(v)] && (next < 0 || sums[size_t(v)] > sums[size_t(next)])) next = v;
+    order.push_back(next);
+    used[size_t(next)] = 1;
+    for (int64_t v = 0; v < n; ++v)
+      if (!used[size_t(v)]) sums[size_t(v)] += sim[size_t(next * n + v)];
+  }
+  return order;
+}
+
 }  // namespace poa
 
 // ---------------------------------------------------------------------------
@@ -488,6 +563,17 @@ int poa_seed_anchor_windows(const poa_params *params, const uint8_t *q, int64_t 
   auto r = anchor_windows(hp, q, qlen, consensus, clen);
   *tail_adaptive = r.second ? 1 : 0;
   return emit(to_c(r.first), out, n_out);
+}
+
+int poa_seed_guide_order(const poa_params *params, int64_t n, const uint8_t *const *seqs, const int64_t *lens,
+                         int64_t **out_order) {
+  HostParams hp;
+  if (!valid_params(params, &hp) || !out_order || n < 0 || (n > 0 && (!seqs || !lens))) return POA_ERR_INVALID;
+  for (int64_t r = 0; r < n; ++r)
+    if (lens[r] < 0 || (lens[r] > 0 && !seqs[r])) return POA_ERR_INVALID;
+  int64_t n_out = 0;
+  return emit(guide_order(hp, std::vector<const uint8_t *>(seqs, seqs + n), std::vector<int64_t>(lens, lens + n)),
+              out_order, &n_out);
 }
 
 }  // extern "C"

@@ -36,5 +36,10 @@ std::pair<std::vector<Anchor>, bool> partition_windows(const std::vector<Anchor>
                                                        int64_t max_drift, int64_t max_win);
 std::pair<std::vector<Anchor>, bool> anchor_windows(const HostParams &p, const uint8_t *q, int64_t qlen,
                                                     const uint8_t *consensus, int64_t clen);
+// Progressive guide order (-p, src/minimizer.rs:505-578): the order in which
+// the reads are added to the graph. The identity unless progressive, with at
+// least two reads and a nucleotide alphabet.
+std::vector<int64_t> guide_order(const HostParams &p, const std::vector<const uint8_t *> &seqs,
+                                 const std::vector<int64_t> &lens);
 
 }  // namespace poa

@@ -9,5 +9,5 @@ Server admits read sets as they arrive (continuous batching).
 from .params import AlignedBase, CParams, Params, Sequence, default_matrix  # noqa: F401
 from .api import (  # noqa: F401
     Anchor, Batch, Context, Graph, Minimizer, PoaError, Server, align, anchor_windows, chain, collect_anchors,
-    partition_windows, repeat_intervals, sketch, align_sequences, default_context, dp_backend, extend_graph, int_peak, poa, read_gfa, run,
+    partition_windows, repeat_intervals, sketch, guide_order, align_sequences, default_context, dp_backend, extend_graph, int_peak, poa, read_gfa, run,
 )

@@ -59,7 +59,7 @@ class BatchStats(ctypes.Structure):
 
 
 class BatchTuning(ctypes.Structure):
-    _fields_ = [("warps_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32), ("giant_factor", ctypes.c_double),
+    _fields_ = [("warps_per_sm", ctypes.c_int32), ("giant_alone", ctypes.c_int32), ("giant_factor", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("trials", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
 
 
@@ -127,6 +127,7 @@ SIGNATURES = {
     "poa_seed_partition_windows": (ctypes.c_int, [P(AnchorC), _i64, _i64, _i64, _i64, _i64, P(P(AnchorC)), P(_i64),
                                                   P(_i32)]),
     "poa_seed_anchor_windows": (ctypes.c_int, [_cp, _u8p, _i64, _u8p, _i64, P(P(AnchorC)), P(_i64), P(_i32)]),
+    "poa_seed_guide_order": (ctypes.c_int, [_cp, _i64, P(_u8p), P(_i64), P(P(_i64))]),
     "poa_server_destroy": (None, [_vp]),
 }
 

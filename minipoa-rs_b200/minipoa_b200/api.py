@@ -602,3 +602,14 @@ def anchor_windows(params: Params, query: bytes, consensus: bytes) -> Tuple[List
     _check(L.poa_seed_anchor_windows(ctypes.byref(c), q, len(query), t, len(consensus), ctypes.byref(out),
                                      ctypes.byref(n), ctypes.byref(tail)))
     return _take(L, out, n.value, _anchor), bool(tail.value)
+
+
+def guide_order(params: Params, reads: Seq[bytes]) -> List[int]:
+    """minimizer::guide_order (src/minimizer.rs:505-578): the order in which
+    progressive alignment (params.progressive, -p) adds the reads."""
+    L = _lib.load()
+    c, _k = params.to_c()
+    arr, lens, _bufs = _seq_arrays(reads)
+    out = ctypes.POINTER(ctypes.c_int64)()
+    _check(L.poa_seed_guide_order(ctypes.byref(c), len(reads), arr, lens, ctypes.byref(out)))
+    return _take(L, out, len(reads), int)

@@ -70,6 +70,9 @@ const char *orc_last_error(void);
 /* lib.rs:177 / lib.rs:184 */
 int orc_align_sequences(const orc_params *p, int64_t n, const uint8_t *const *seqs, const int64_t *lens,
                         int kernel, void **out_graph);
+/* align_sequences with progressive guide order: the reads in `order` */
+int orc_align_sequences_in_order(const orc_params *p, int64_t n, const uint8_t *const *seqs, const int64_t *lens,
+                                 const int64_t *order, int kernel, void **out_graph);
 int orc_extend_graph(const orc_params *p, void *g, int64_t n, const uint8_t *const *seqs, const int64_t *lens,
                      int64_t existing, int kernel);
 /* align.rs:81 */

@@ -65,6 +65,8 @@ def lib():
         L.orc_last_error.restype = ctypes.c_char_p
         L.orc_align_sequences.argtypes = [cp, i64, P(P(ctypes.c_uint8)), P(i64), ctypes.c_int, P(vp)]
         L.orc_extend_graph.argtypes = [cp, vp, i64, P(P(ctypes.c_uint8)), P(i64), i64, ctypes.c_int]
+        L.orc_align_sequences_in_order.argtypes = [cp, i64, P(P(ctypes.c_uint8)), P(i64), P(i64), ctypes.c_int,
+                                                   P(vp)]
         L.orc_align.argtypes = [cp, vp, P(ctypes.c_uint8), i64, ctypes.c_int, P(P(_Item)), P(i64)]
         L.orc_poa.argtypes = [cp, vp, i64, i64, P(ctypes.c_uint8), i64, ctypes.c_int, u64, ctypes.c_int,
                               ctypes.c_int, P(P(_Item)), P(i64)]
@@ -305,6 +307,19 @@ def align_sequences(params, seqs: Seq[bytes], kernel=AUTO_SERIAL) -> OracleGraph
     arr, lens, bufs = _seqs(seqs)
     out = ctypes.c_void_p()
     _check(lib().orc_align_sequences(ctypes.byref(c), len(seqs), arr, lens, kernel, ctypes.byref(out)))
+    return OracleGraph(handle=out.value)
+
+
+def align_sequences_in_order(params, seqs: Seq[bytes], order: Seq[int], kernel=AUTO_SERIAL) -> OracleGraph:
+    """lib.rs:177 with progressive (-p): the reads added in `order` (the
+    guide order, src/minimizer.rs:505-578, computed from the same sketches
+    as the GPU path's)."""
+    c, keep = _params(params)
+    arr, lens, bufs = _seqs(seqs)
+    od = (ctypes.c_int64 * max(1, len(order)))(*order)
+    out = ctypes.c_void_p()
+    _check(lib().orc_align_sequences_in_order(ctypes.byref(c), len(seqs), arr, lens, od, kernel,
+                                              ctypes.byref(out)))
     return OracleGraph(handle=out.value)
 
 

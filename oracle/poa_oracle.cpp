@@ -1038,11 +1038,17 @@ static std::vector<AlignedBase> align(const Params &params, const Graph &graph, 
   return poa(params, graph, 0, 1, q, qlen, params.adaptive, params.b, kernel);
 }
 
-// lib.rs:184-204 (progressive guide order is not restated here)
+// lib.rs:184-204. With progressive (-p) the reads go in the guide order
+// (minimizer::guide_order, src/minimizer.rs:505-578), which depends on the
+// minimizer sketches: the caller passes it (`order`, n entries), as the
+// GPU path computes it, so both align the reads in the same order; paths
+// keep each read's own index.
 static void extend_graph(const Params &params, Graph &graph, usize n, const uint8_t *const *seqs, const int64_t *lens,
-                         usize existing, int kernel) {
-  if (params.progressive && existing == 0) throw Error("progressive guide order is not available in this build");
-  for (usize id = existing; id < n; ++id) {
+                         usize existing, int kernel, const int64_t *order = nullptr) {
+  if (params.progressive && existing == 0 && !order)
+    throw Error("progressive guide order needs the order (the sketches are the library's)");
+  for (usize k = existing; k < n; ++k) {
+    const usize id = (order && existing == 0) ? usize(order[k]) : k;
     auto path = align(params, graph, seqs[id], usize(lens[id]), kernel);
     graph.add_path(id, path);
     graph.toposort(false);
@@ -1239,6 +1245,23 @@ int orc_align_sequences(const orc_params *p, int64_t n, const uint8_t *const *se
     auto *g = new Graph(pp);
     try {
       extend_graph(pp, *g, usize(n), seqs, lens, 0, kernel);
+    } catch (...) {
+      delete g;
+      throw;
+    }
+    *out_graph = g;
+  });
+}
+
+int orc_align_sequences_in_order(const orc_params *p, int64_t n, const uint8_t *const *seqs, const int64_t *lens,
+                                 const int64_t *order, int kernel, void **out_graph) {
+  *out_graph = nullptr;
+  return guard([&] {
+    Params pp = Params::from(p);
+    pp.validate();
+    auto *g = new Graph(pp);
+    try {
+      extend_graph(pp, *g, usize(n), seqs, lens, 0, kernel, order);
     } catch (...) {
       delete g;
       throw;

@@ -25,7 +25,8 @@ def test_autotune_caches_a_setting_and_keeps_the_bytes(tmp_path, monkeypatch):
     b.run(0)
     want = b.output_all(2)
     t = b.autotune()
-    assert t.trials == 5 and t.warps_per_sm in (4, 6, 8) and t.giant_factor in (0.0, 1.5, 3.0)
+    assert t.trials == 7 and t.warps_per_sm in (4, 6, 8) and t.giant_factor in (0.0, 1.5, 3.0)
+    assert t.giant_alone in (0, 1)
     assert b.output_all(2) == want
     b.run(0)
     assert b.output_all(2) == want
@@ -35,6 +36,7 @@ def test_autotune_caches_a_setting_and_keeps_the_bytes(tmp_path, monkeypatch):
     b2 = mp.Batch(params, sets)  # same size bucket: the cached setting applies
     tt = b2.tuning()
     assert tt.warps_per_sm == t.warps_per_sm and tt.giant_factor == t.giant_factor
+    assert tt.giant_alone == t.giant_alone
     b2.run(0)
     assert b2.output_all(2) == want
     os.unlink(tmp_path / "tune.tsv")

@@ -125,3 +125,83 @@ def test_seeded_windows_of_a_mutated_read_are_ordered():
     for a in anchors:
         assert a.target_end - a.span + 1 > prev_t and a.query_end - a.span + 1 > prev_q
         prev_t, prev_q = a.target_end, a.query_end
+
+
+def _guide_order_restated(params, seqs):
+    """src/minimizer.rs:505-578 over this library's sketches, in Python: the
+    independent check of the similarity arithmetic and the greedy order."""
+    n = len(seqs)
+    if not params.progressive or n < 2 or len(params.alphabet) > 5:
+        return list(range(n))
+    groups = {}
+    for rid, s in enumerate(seqs):
+        for m in mp.sketch(s, params.k, params.w):
+            counts = groups.setdefault(m.value, {})
+            counts[rid] = counts.get(rid, 0) + 1
+    if not groups:
+        return list(range(n))
+    total = [0] * n
+    shared = [0] * (n * n)
+    for value in sorted(groups):
+        counts = groups[value]
+        if len(counts) > n * params.mm_filter_ratio:
+            continue
+        keys = sorted(counts)
+        for ia, a in enumerate(keys):
+            total[a] += counts[a]
+            for b in keys[:ia]:
+                m = min(counts[a], counts[b])
+                shared[a * n + b] += m
+                shared[b * n + a] += m
+    max_len = float(max(1, max(len(s) for s in seqs)))
+    sim = [0.0] * (n * n)
+    best = (-1.0, 0, 1)
+    for i in range(n):
+        for j in range(n):
+            if i == j:
+                continue
+            common = shared[i * n + j]
+            union = total[i] + total[j] - common
+            jac = 0.0 if union == 0 else common / union * (0.51 * len(seqs[i]) / max_len + 0.49 * len(seqs[j]) / max_len)
+            sim[i * n + j] = jac
+            if jac > best[0]:
+                best = (jac, i, j)
+    order = [best[1], best[2]]
+    used = [False] * n
+    used[best[1]] = used[best[2]] = True
+    sums = [sim[best[1] * n + v] + sim[best[2] * n + v] for v in range(n)]
+    while len(order) < n:
+        nxt = max((v for v in range(n) if not used[v]), key=lambda v: (sums[v], -v))
+        order.append(nxt)
+        used[nxt] = True
+        for v in range(n):
+            if not used[v]:
+                sums[v] += sim[nxt * n + v]
+    return order
+
+
+def test_guide_order_is_permutation_and_deterministic():
+    # src/minimizer.rs:746-772
+    seqs = [random_dna(600 + i) for i in range(12)]
+    p = Params(progressive=True)
+    order = mp.guide_order(p, seqs)
+    assert order == mp.guide_order(p, seqs)
+    assert sorted(order) == list(range(len(seqs)))
+    assert mp.guide_order(p, [b"ACGT"] * 3) == [0, 1, 2]
+    assert mp.guide_order(Params(), seqs) == list(range(len(seqs)))  # not progressive
+
+
+def test_guide_order_arithmetic_matches_a_restatement():
+    rng = np.random.default_rng(505)
+    from minipoa_b200 import workloads
+
+    p = Params(progressive=True)
+    for trial in range(4):
+        anc = int(rng.integers(300, 900))
+        reads = workloads.read_set(rng, anc, int(rng.integers(4, 14)), 0.03 * trial, 0.01 * trial, 0.01 * trial)
+        # unrelated reads too, so that some pairs share nothing
+        reads += [random_dna(200 + 37 * trial)[::-1]]
+        assert mp.guide_order(p, reads) == _guide_order_restated(p, reads)
+    prot = Params(progressive=True, alphabet=b"ACDEFGHIKLMNPQRSTVWYX",
+                  matrix=[1 if i == j else 0 for i in range(21) for j in range(21)])
+    assert mp.guide_order(prot, [b"ACD", b"CDE", b"DEF"]) == [0, 1, 2]  # protein: input order
