@@ -319,8 +319,10 @@ typedef struct poa_batch_tuning {
 int poa_batch_autotune(poa_ctx *ctx, poa_batch *batch, poa_batch_tuning *out);
 int poa_batch_tuning_get(poa_ctx *ctx, poa_batch *batch, poa_batch_tuning *out);
 
-/* Tuning: concurrent warp slots per SM for the batched kernel (0 = auto) and
- * the DP arena bytes per slot (0 = auto from the budget). */
+/* Tuning: warp slots per SM for the batched kernel (0 = 6, the untuned
+ * default; poa_batch_create applies a cached tuned setting first; up to 8
+ * are resident at once, more only add slots that start when others leave)
+ * and the DP arena bytes per slot (0 = auto from the budget). */
 int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot);
 
 /* ---- serving loop (no reference counterpart: the reference is a CLI that

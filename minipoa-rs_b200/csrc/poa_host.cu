@@ -880,6 +880,12 @@ std::vector<std::string> name_list(int64_t n, const char *const *names, const ch
 // ---------------------------------------------------------------------------
 // Batch of independent read sets.
 
+// Resident warps per SM of a batched run without a tuned setting: 6 of the
+// kernel's 8 (the largest sets, which end the run, slow down when their SM
+// also runs four other jobs; measured 3.5-3.6 s per C3 step at 6 or 4 warps
+// per SM against 4.0-4.2 s at 8).
+constexpr int kDefaultBatchWarpsPerSm = 6;
+
 struct poa_batch {
   poa_ctx *ctx = nullptr;
   HostParams hp;
@@ -1636,7 +1642,8 @@ int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
       double gf;
       int alone;
     };
-    const Cand cand[] = {{8, 1.5, 0}, {8, 1.5, 1}, {8, 3.0, 1}, {6, 1.5, 0}, {4, 1.5, 0}, {4, 3.0, 0}, {8, 0.0, 0}};
+    const Cand cand[] = {{kDefaultBatchWarpsPerSm, 1.5, 0}, {6, 1.5, 1}, {4, 1.5, 0}, {5, 1.5, 0},
+                         {7, 1.5, 0},  {8, 1.5, 0},  {8, 1.5, 1}, {6, 3.0, 0}};
     double best_ms = 0;
     Cand best{b->warps_per_sm, b->giant_factor, b->giant_alone};
     int tried = 0;
@@ -1673,7 +1680,7 @@ int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
 
 int poa_batch_tuning_get(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
   return api(ctx, [&] {
-    out->warps_per_sm = b->warps_per_sm > 0 ? b->warps_per_sm : batch_resident_warps_per_sm();
+    out->warps_per_sm = b->warps_per_sm > 0 ? b->warps_per_sm : kDefaultBatchWarpsPerSm;
     out->giant_alone = b->giant_alone;
     out->giant_factor = b->giant_factor;
     out->device_ms = 0;
@@ -1683,6 +1690,7 @@ int poa_batch_tuning_get(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
 
 int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_t arena_bytes_per_slot) {
   return api(ctx, [&] {
+    if (warps_per_sm < 0) throw AlignError{POA_ERR_INVALID, "warps per SM must not be negative"};
     batch->warps_per_sm = warps_per_sm;
     batch->slot_bytes_override = arena_bytes_per_slot;
   });
@@ -1703,7 +1711,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
       b->arena_pool = pool;
     }
     const int sms = ctx->sm_count;
-    int wps = b->warps_per_sm > 0 ? b->warps_per_sm : batch_resident_warps_per_sm();
+    int wps = b->warps_per_sm > 0 ? b->warps_per_sm : kDefaultBatchWarpsPerSm;
     int passes = 0, launches = 0;
     double kernel_ms = 0;
     CK(cudaEventRecord(b->e0, ctx->stream));

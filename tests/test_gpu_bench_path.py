@@ -87,6 +87,7 @@ def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive, dp)
     sets = _full_machine_sets(2024 + int(adaptive), 4, 4200, 30, 1180)
     with _dp_rows(dp):
         batch = mp.Batch(params, sets)
+    batch.tune(8)  # full 8-warp blocks: the giant runs on warp 4 with warps 0-2 as helpers
     st = batch.run(0)
     # one slot per resident warp of every SM in the first pass: full 8-warp
     # blocks (an adaptive giant may outgrow its arena and finish in a second
