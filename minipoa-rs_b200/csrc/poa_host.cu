@@ -606,15 +606,17 @@ void extend_range(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::v
   }
   g->reserve(total + 2 * (n - r0), 2 * (total + 3 * (n - r0)), total + (n - r0), n - r0);
   DevParams P = ctx->params(hp);
-  // reads, offsets, lengths and sequence ids in one upload
+  // scheduler words of the one-job launch, then reads, offsets, lengths and
+  // sequence ids, in one upload
+  const size_t sched_bytes = ((4 + sched_words(1)) * 4 + 255) / 256 * 256;
   const size_t off_bytes = size_t(n) * 8, len_bytes = size_t(n) * 4, id_bytes = size_t(n) * 4;
-  const size_t need = off_bytes + len_bytes + id_bytes + size_t(std::max<int64_t>(total, 1)) + 64;
+  const size_t need = sched_bytes + off_bytes + len_bytes + id_bytes + size_t(std::max<int64_t>(total, 1)) + 64;
   ctx->ensure_qbuf(need);
   std::vector<uint8_t> host(need);
-  int64_t *off = (int64_t *)host.data();
-  int32_t *ln = (int32_t *)(host.data() + off_bytes);
-  int32_t *ids = (int32_t *)(host.data() + off_bytes + len_bytes);
-  uint8_t *rd = host.data() + off_bytes + len_bytes + id_bytes;
+  int64_t *off = (int64_t *)(host.data() + sched_bytes);
+  int32_t *ln = (int32_t *)(host.data() + sched_bytes + off_bytes);
+  int32_t *ids = (int32_t *)(host.data() + sched_bytes + off_bytes + len_bytes);
+  uint8_t *rd = host.data() + sched_bytes + off_bytes + len_bytes + id_bytes;
   int64_t at = 0;
   for (int64_t r = 0; r < n; ++r) {
     off[r] = at;
@@ -624,39 +626,58 @@ void extend_range(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::v
     if (r >= r0) at += lens[r];
   }
   CK(cudaMemcpyAsync(ctx->qbuf, host.data(), need, cudaMemcpyHostToDevice, ctx->stream));
-  const int64_t *d_off = (const int64_t *)ctx->qbuf;
-  const int32_t *d_len = (const int32_t *)(ctx->qbuf + off_bytes);
-  const int32_t *d_ids = (const int32_t *)(ctx->qbuf + off_bytes + len_bytes);
-  const uint8_t *d_rd = ctx->qbuf + off_bytes + len_bytes + id_bytes;
-  // the device advances next_read after each completed read
+  int32_t *d_sched = (int32_t *)ctx->qbuf;
+  const int64_t *d_off = (const int64_t *)(ctx->qbuf + sched_bytes);
+  const int32_t *d_len = (const int32_t *)(ctx->qbuf + sched_bytes + off_bytes);
+  const int32_t *d_ids = (const int32_t *)(ctx->qbuf + sched_bytes + off_bytes + len_bytes);
+  const uint8_t *d_rd = ctx->qbuf + sched_bytes + off_bytes + len_bytes + id_bytes;
+  // The batched kernel runs the read loop as one job in a 4-warp block, the
+  // job marked giant so the other three warps compute its DP rows with it;
+  // the device advances next_read after each completed read. The job's
+  // descriptor names its reads and its arena for the launch.
   g->sync();
+  g->h.reads = d_rd;
+  g->h.read_off = d_off;
+  g->h.read_len = d_len;
+  g->h.n_reads = int32_t(n);
   g->h.next_read = int32_t(r0);
-  g->h.status = ST_OK;
   g->h.read_id = ordered ? d_ids : nullptr;
-  g->upload();
+  g->h.giant = 1;
+  g->h.done_flag = nullptr;
   // initial arena: scratch + a static-band estimate, grown on ARENA_FULL
   int64_t arena = std::max<int64_t>(int64_t(64) << 20, ctx->arena_bytes);
-  int64_t r = r0;
+  auto detach = [&] {  // the descriptor as the other single-graph calls expect it
+    g->h.status = ST_OK;
+    g->h.arena = nullptr;
+    g->h.arena_bytes = 0;
+    g->h.read_id = nullptr;
+    g->h.giant = 0;
+    g->upload();
+  };
   for (;;) {
     ctx->ensure_arena(arena);
-    CK(launch_extend_range(g->d_job, P, ctx->arena, ctx->arena_bytes, d_rd, d_off, d_len, int(r), int(n),
-                           ctx->stream));
+    g->h.arena = ctx->arena;
+    g->h.arena_bytes = ctx->arena_bytes;
+    g->h.status = ST_OK;
+    g->upload();
+    CK(cudaMemsetAsync(d_sched, 0, sched_bytes, ctx->stream));
+    CK(launch_single(g->d_job, d_sched, ctx->sm_count, P, ctx->stream));
     g->sync();
-    if (g->h.status == ST_OK) break;
     const int32_t st = g->h.status;
+    if (st == ST_OK) break;
     if (st == ST_ARENA_FULL) {
-      r = g->h.next_read;
-      g->h.status = ST_OK;
-      g->upload();
-      if (arena >= int64_t(ctx->budget)) throw AlignError{POA_ERR_ALLOC, "DP arena exceeds the memory budget"};
+      if (arena >= int64_t(ctx->budget)) {
+        detach();
+        throw AlignError{POA_ERR_ALLOC, "DP arena exceeds the memory budget"};
+      }
       arena = std::min<int64_t>(arena * 2, int64_t(ctx->budget - std::min(ctx->budget, ctx->allocated)) +
                                                ctx->arena_bytes);
       continue;
     }
-    g->h.status = ST_OK;
-    g->upload();
+    detach();
     throw AlignError{status_code(st), status_message(st, g->h.err_i, g->h.err_j)};
   }
+  detach();
 }
 
 // align / poa on a graph without changing it.

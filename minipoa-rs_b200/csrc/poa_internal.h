@@ -21,6 +21,12 @@ cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, 
                          const DevParams &P, char *arenas, int64_t slot_bytes, int slots, cudaStream_t stream);
 cudaError_t launch_extend_step(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, int read,
                                cudaStream_t stream);
+// The read loop of one job (its remaining reads, then the exact rank order)
+// by the batched kernel in one 4-warp block: a job marked giant gets the
+// other three warps as helpers for its DP rows. `order_sched` holds
+// 4 + sched_words(1) zeroed int32 words (the queue order [0], then the
+// scheduler words); the job's descriptor names its reads and its arena.
+cudaError_t launch_single(Job *job_dev, int32_t *order_sched, int num_sms, const DevParams &P, cudaStream_t stream);
 cudaError_t launch_extend_range(Job *job_dev, const DevParams &P, char *arena, int64_t bytes, const uint8_t *reads,
                                 const int64_t *read_off, const int32_t *read_len, int r0, int r1,
                                 cudaStream_t stream);

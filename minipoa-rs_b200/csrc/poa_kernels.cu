@@ -192,6 +192,19 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
       first_giant = 0;
     }
   }
+  if (block_giant == 1 && wpb == 4 && int64_t(blockIdx.x) * wpb < slots) {
+    // a 4-warp block (a single job run with helpers): the giant runs on warp
+    // 0 with warps 1-3 as helpers, whichever warp drew it
+    lead = 0;
+    h0 = 1;
+    if (me == 0 && giant_warp != 0) {
+      first = firsts[giant_warp];
+      first_giant = 1;
+    } else if (me == giant_warp && giant_warp != 0) {
+      first = firsts[0];
+      first_giant = 0;
+    }
+  }
   const bool coop_block = block_giant == 1 && h0 >= 0;
   if (coop_block && me >= h0 && me < h0 + 3) {
     WarpSmem *leader = reinterpret_cast<WarpSmem *>(sm) - me + lead;
@@ -422,6 +435,14 @@ cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, 
   if (pe != cudaSuccess) return pe;
   k_batch<<<blocks, wpb * 32, wpb * sizeof(WarpSmem), stream>>>(const_cast<Job *>(jobs_dev), order, n_jobs, sched,
                                                                 num_sms, P, arenas, slot_bytes, slots, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_single(Job *job_dev, int32_t *order_sched, int num_sms, const DevParams &P, cudaStream_t stream) {
+  const cudaError_t pe = prepare_batch_kernel();
+  if (pe != cudaSuccess) return pe;
+  k_batch<<<1, 4 * 32, 4 * sizeof(WarpSmem), stream>>>(job_dev, order_sched, 1, order_sched + 4, num_sms, P, nullptr,
+                                                       0, 4, nullptr);
   return cudaGetLastError();
 }
 
