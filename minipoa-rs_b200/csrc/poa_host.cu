@@ -37,6 +37,10 @@ struct CudaError {
   std::string where;
 };
 
+inline double now_steady() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 #define CK(call)                                                   \
   do {                                                             \
     cudaError_t e_ = (call);                                       \
@@ -182,6 +186,8 @@ struct poa_ctx {
   int64_t arena_bytes = 0;
   uint8_t *qbuf = nullptr;
   size_t qbuf_bytes = 0;
+  char *dlbuf = nullptr;  // graph downloads: packed records (grow-only, reused)
+  size_t dlbuf_bytes = 0;
   int4 *items = nullptr;
   int32_t *n_items = nullptr;
   size_t items_cap = 0;
@@ -227,6 +233,14 @@ struct poa_ctx {
     qbuf_bytes = 0;
     qbuf = (uint8_t *)dalloc(bytes);
     qbuf_bytes = bytes;
+  }
+  void ensure_dlbuf(size_t bytes) {
+    if (dlbuf_bytes >= bytes) return;
+    dfree(dlbuf, dlbuf_bytes);
+    dlbuf = nullptr;
+    dlbuf_bytes = 0;
+    dlbuf = (char *)dalloc(bytes);
+    dlbuf_bytes = bytes;
   }
   void ensure_items(size_t n) {
     if (items_cap >= n) return;
@@ -369,27 +383,17 @@ struct poa_graph {
   HostGraph download() {
     sync();
     const int64_t words = packed_words(h, sigma);
-    int32_t *d_out = (int32_t *)ctx->dalloc(size_t(words) * 4 + 16);
-    int64_t *d_off = (int64_t *)ctx->dalloc(16);
-    int32_t *d_id = (int32_t *)ctx->dalloc(16);
+    // the context's download buffer (grown, never freed per call: a
+    // cudaFree would synchronise the device on every download)
+    ctx->ensure_dlbuf(size_t(words) * 4 + 256);
+    int64_t *d_off = reinterpret_cast<int64_t *>(ctx->dlbuf);
+    int32_t *d_id = reinterpret_cast<int32_t *>(ctx->dlbuf + 16);
+    int32_t *d_out = reinterpret_cast<int32_t *>(ctx->dlbuf + 256);
     std::vector<int32_t> rec(static_cast<size_t>(words));
-    try {
-      const int64_t zero = 0;
-      const int32_t zid = 0;
-      CK(cudaMemcpyAsync(d_off, &zero, 8, cudaMemcpyHostToDevice, ctx->stream));
-      CK(cudaMemcpyAsync(d_id, &zid, 4, cudaMemcpyHostToDevice, ctx->stream));
-      CK(launch_pack(d_job, d_id, 1, d_off, d_out, sigma, ctx->stream));
-      CK(cudaMemcpyAsync(rec.data(), d_out, size_t(words) * 4, cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-    } catch (...) {
-      ctx->dfree(d_out, size_t(words) * 4 + 16);
-      ctx->dfree(d_off, 16);
-      ctx->dfree(d_id, 16);
-      throw;
-    }
-    ctx->dfree(d_out, size_t(words) * 4 + 16);
-    ctx->dfree(d_off, 16);
-    ctx->dfree(d_id, 16);
+    CK(cudaMemsetAsync(ctx->dlbuf, 0, 32, ctx->stream));  // offset 0, id 0
+    CK(launch_pack(d_job, d_id, 1, d_off, d_out, sigma, ctx->stream));
+    CK(cudaMemcpyAsync(rec.data(), d_out, size_t(words) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return HostGraph::parse(rec.data());
   }
 };
@@ -727,8 +731,26 @@ std::vector<poa_aligned_base> align_path(poa_ctx *ctx, const HostParams &hp, poa
 // window between its anchor nodes (device) and the anchor nodes themselves,
 // in window order. Anchors that are not usable as hard constraints, or no
 // anchors at all, fall back to the whole graph with an adaptive band.
+#ifdef POA_SEED_PROFILE
+// profiling builds: host seconds of the seeded read loop's parts, printed
+// when the process exits
+struct SeedProfile {
+  double download = 0, pack = 0, windows = 0, device = 0, fusion = 0;
+  ~SeedProfile() {
+    std::fprintf(stderr, "seed profile: download+order %.3f s (of it download %.3f s), consensus+windows %.3f s, "
+                 "window DP %.3f s, add_path %.3f s\n", download, pack, windows, device, fusion);
+  }
+} g_seed_prof;
+#define SEED_T(name) const double name = now_steady()
+#define SEED_ADD(field, a, b) g_seed_prof.field += (b) - (a)
+#else
+#define SEED_T(name) (void)0
+#define SEED_ADD(field, a, b) (void)0
+#endif
+
 std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const uint8_t *q,
                                            int64_t len, bool ranks_stale = false) {
+  SEED_T(t0);
   g->sync();
   std::vector<poa_aligned_base> out;
   if (g->h.n_nodes <= 2) {
@@ -736,7 +758,10 @@ std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, p
     for (int64_t c = 0; c < len; ++c) out.push_back({-1, hp.encode(q[c]), -1});
     return out;
   }
+  SEED_T(tp0);
   HostGraph hg = g->download();
+  SEED_T(tp1);
+  SEED_ADD(pack, tp0, tp1);
   if (ranks_stale) {
     // the previous read's toposort (graph.rs:125-178), on the downloaded copy
     const int32_t st = hg.lifo_order();
@@ -749,10 +774,14 @@ std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, p
     g->h.order_exact = 1;
     g->upload();
   }
+  SEED_T(t1);
+  SEED_ADD(download, t0, t1);
   std::vector<uint8_t> cons;
   std::vector<int64_t> ids, cov;
   hg.consensus(hp, cons, ids, cov);
   const auto aw = anchor_windows(hp, q, len, cons.data(), int64_t(cons.size()));
+  SEED_T(t2);
+  SEED_ADD(windows, t1, t2);
   auto whole = [&] {
     ++ctx->seed_fallbacks;
     ++ctx->seed_launches;
@@ -844,6 +873,8 @@ std::vector<poa_aligned_base> seeded_align(poa_ctx *ctx, const HostParams &hp, p
     parts[size_t(k)] = align_path(ctx, hp, g, q + w.qbeg, w.qend - w.qbeg, 1, w.beg, w.end, w.adaptive ? 1 : 0,
                                   w.adaptive ? hp.b : hp.win_band, 0, 1);
   }
+  SEED_T(t3);
+  SEED_ADD(device, t2, t3);
   for (int k = 0; k < nw; ++k) {
     const Window &w = windows[size_t(k)];
     out.insert(out.end(), parts[size_t(k)].begin(), parts[size_t(k)].end());
@@ -873,14 +904,20 @@ void seeded_extend(poa_ctx *ctx, const HostParams &hp, poa_graph *g, const std::
   for (int64_t k = r0; k < n; ++k) {
     const int64_t r = order.empty() ? k : order[size_t(k)];
     auto path = seeded_align(ctx, hp, g, seqs[size_t(r)], lens[size_t(r)], stale);
+    SEED_T(ta);
     std::vector<int4> it(path.size());
     for (size_t k = 0; k < path.size(); ++k)
       it[k] = make_int4(int(path[k].node), int(path[k].base), int(path[k].aligned), 0);
     ctx->ensure_items(it.size() + 4);
     if (!it.empty())
       CK(cudaMemcpyAsync(ctx->items, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
-    CK(launch_add_path(g->d_job, P, int(r), ctx->items, int(it.size()), ctx->stream));
+    // scratch for add_path's node marks (n_nodes words)
+    ctx->ensure_arena(std::max<int64_t>(int64_t(g->h.n_nodes) * 4 + 256, ctx->arena_bytes));
+    CK(launch_add_path(g->d_job, P, int(r), ctx->items, int(it.size()), ctx->stream,
+                       reinterpret_cast<int32_t *>(ctx->arena)));
     g->check_status();
+    SEED_T(tb);
+    SEED_ADD(fusion, ta, tb);
     stale = true;
   }
   if (stale) {
@@ -1152,6 +1189,7 @@ void poa_ctx_destroy(poa_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->dfree(ctx->arena, size_t(ctx->arena_bytes));
   ctx->dfree(ctx->qbuf, ctx->qbuf_bytes);
+  ctx->dfree(ctx->dlbuf, ctx->dlbuf_bytes);
   ctx->dfree(ctx->items, 0);
   ctx->dfree(ctx->d_matrix, 0);
   ctx->dfree(ctx->d_encode, 0);

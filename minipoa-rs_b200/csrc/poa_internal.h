@@ -37,8 +37,11 @@ cudaError_t launch_align(Job *job_dev, const DevParams &P, char *arena, int64_t 
 cudaError_t launch_windows(Job *job_dev, const DevParams &P, char *arenas, int64_t slot_bytes, int n_win,
                            const int4 *win, const uint64_t *band, const uint8_t *query, int4 *items,
                            const int64_t *item_off, int32_t *out_n, int32_t *out_st, cudaStream_t stream);
+// mark: n_nodes words of scratch for the warp path's distinct-node check
+// (nullptr: nodes must come in strictly increasing rank order, else the
+// serial add_path runs)
 cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, int4 *items, int n,
-                            cudaStream_t stream);
+                            cudaStream_t stream, int32_t *mark = nullptr);
 cudaError_t launch_add_node(Job *job_dev, int sigma, int base, cudaStream_t stream);
 cudaError_t launch_add_edge(Job *job_dev, int from, int to, cudaStream_t stream);
 cudaError_t launch_toposort(Job *job_dev, char *arena, int64_t bytes, cudaStream_t stream);

@@ -366,9 +366,9 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   }
 }
 
-__global__ void k_add_path(Job *J, DevParams P, int seq_id, int4 *items, int n) {
+__global__ void k_add_path(Job *J, DevParams P, int seq_id, int4 *items, int n, int32_t *mark) {
   int32_t st = ST_OK;
-  if (!add_path_warp(J, P, seq_id, items, n, &st) && threadIdx.x == 0) st = add_path(J, P, seq_id, items, n);
+  if (!add_path_warp(J, P, seq_id, items, n, &st, mark) && threadIdx.x == 0) st = add_path(J, P, seq_id, items, n);
   if (threadIdx.x == 0) J->status = st;
 }
 
@@ -487,8 +487,8 @@ cudaError_t launch_windows(Job *job_dev, const DevParams &P, char *arenas, int64
 }
 
 cudaError_t launch_add_path(Job *job_dev, const DevParams &P, int seq_id, int4 *items, int n,
-                            cudaStream_t stream) {
-  k_add_path<<<1, 32, 0, stream>>>(job_dev, P, seq_id, items, n);
+                            cudaStream_t stream, int32_t *mark) {
+  k_add_path<<<1, 32, 0, stream>>>(job_dev, P, seq_id, items, n, mark);
   return cudaGetLastError();
 }
 
