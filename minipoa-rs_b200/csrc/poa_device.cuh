@@ -1292,7 +1292,9 @@ __device__ inline bool i32_scores_safe(const Job *J, const DevParams &P, int beg
 // rows of the widest bands kept here, ten of 256 columns). Also the scoring
 // matrix, the guide-pass rings and the encoded query (one byte per column).
 constexpr int RING_CAP = 2560;
-constexpr int RING_MAX_LEN = 512;  // widest band computed by the striped row
+constexpr int RING_MAX_LEN = 512;   // widest band computed by one striped tile (4 stripes)
+constexpr int RING_WIDE_LEN = 2048; // widest band computed by striped tiles in segments
+static_assert(RING_WIDE_LEN <= RING_CAP, "a ring row must fit the ring");
 constexpr int SMEM_MATRIX = 512;   // sigma^2 entries kept in shared memory (sigma <= 22)
 constexpr int SEQ_SMEM = 5632;     // padded query columns kept in shared memory
 // Where a warp's ring lives: its own ring_m / ring_d by default; a warp
@@ -1345,13 +1347,19 @@ __device__ __forceinline__ int ring_at(int pos, int start, int j, int cap) {
 // with I[start] = NEG32. The stripe loops are branch-free (loads go to a
 // clamped, in-bounds column and the value is then selected) so the compiler
 // can overlap the stripes' dependency chains.
-template <int G, bool ADAPT>
+// SEG: the tile is one segment of a row wider than 4 stripes, at column
+// offset c0 of the row: its insertion state enters from `carry_io` (the
+// state leaving the previous segment's last column) and leaves there, and
+// the ring entries are written by the caller once every segment has read its
+// predecessors.
+template <int G, bool ADAPT, bool SEG = false>
 __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                                const int32_t *mrow, int32_t E, int32_t O, unsigned vmask,
                                                int my_ps, int my_pl, int my_pos, const int32_t *my_g,
                                                int32_t *rm, int32_t *rd, int cap, int pos_i, int32_t &bestv,
-                                               int &bestj) {
+                                               int &bestj, int c0 = 0, int32_t *carry_io = nullptr) {
   const int stop = start + len;
+  const int cs = SEG ? start + c0 : start;  // first column of the tile
   int32_t Mx[G][4], Dx[G][4];
 #pragma unroll
   for (int g = 0; g < G; ++g)
@@ -1372,7 +1380,7 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
     if (pos >= 0) {
 #pragma unroll
       for (int g = 0; g < G; ++g) {
-        const int j0 = start + 128 * g + 4 * lane;
+        const int j0 = cs + 128 * g + 4 * lane;
         in[g] = j0 < stop && j0 >= ps && j0 < ps + pl;
         const int x = ring_at(pos, ps, in[g] ? j0 : ps, cap);
         m4[g] = *reinterpret_cast<const int4 *>(rm + x);
@@ -1384,7 +1392,7 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
       const int32_t *gp = reinterpret_cast<const int32_t *>(__shfl_sync(FULL, (long long)my_g, t));
 #pragma unroll
       for (int g = 0; g < G; ++g) {
-        const int j0 = start + 128 * g + 4 * lane;
+        const int j0 = cs + 128 * g + 4 * lane;
         in[g] = j0 < stop && j0 >= ps && j0 < ps + pl;
         const int c = in[g] ? j0 - ps : 0;
         m4[g] = *reinterpret_cast<const int4 *>(gp + c);
@@ -1394,7 +1402,7 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
     }
 #pragma unroll
     for (int g = 0; g < G; ++g) {
-      const int j0 = start + 128 * g + 4 * lane;
+      const int j0 = cs + 128 * g + 4 * lane;
       const int32_t pv = j0 > ps ? prev[g] : NEG32;
       if (in[g]) {
         Mx[g][0] = maxs(Mx[g][0], pv);
@@ -1417,7 +1425,7 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
   int32_t X[G][4], pre[G];
 #pragma unroll
   for (int g = 0; g < G; ++g) {
-    const int j0 = start + 128 * g + 4 * lane;
+    const int j0 = cs + 128 * g + 4 * lane;
     const uint32_t bw = *reinterpret_cast<const uint32_t *>(seq8 + min(j0, stop - 4));
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -1443,16 +1451,17 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
   // carried-in state is max(pre, carry shifted). The T are independent, so
   // the chain is arithmetic only.
   int32_t cin[G];
-  int32_t carry = NEG32;
+  int32_t carry = SEG ? *carry_io : NEG32;
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     cin[g] = __viaddmax_s32(carry, 4 * lane * E, pre[g]);
-    if (g + 1 < G) carry = __viaddmax_s32(carry, 128 * E, T[g]);
+    if (SEG || g + 1 < G) carry = __viaddmax_s32(carry, 128 * E, T[g]);
   }
+  if (SEG) *carry_io = carry;
   __syncwarp();  // every predecessor read of the ring precedes this row's writes
 #pragma unroll
   for (int g = 0; g < G; ++g) {
-    const int j0 = start + 128 * g + 4 * lane;
+    const int j0 = cs + 128 * g + 4 * lane;
     int32_t iv[4], mv[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -1469,9 +1478,11 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
           }
       }
       const int o = j0 - start;
-      const int x = ring_at(pos_i, start, j0, cap);
-      *reinterpret_cast<int4 *>(rm + x) = make_int4(mv[0], mv[1], mv[2], mv[3]);
-      *reinterpret_cast<int4 *>(rd + x) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
+      if (!SEG) {
+        const int x = ring_at(pos_i, start, j0, cap);
+        *reinterpret_cast<int4 *>(rm + x) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+        *reinterpret_cast<int4 *>(rd + x) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
+      }
       *reinterpret_cast<int4 *>(R + o) = make_int4(mv[0], mv[1], mv[2], mv[3]);
       *reinterpret_cast<int4 *>(R + len + o) = make_int4(Dx[g][0], Dx[g][1], Dx[g][2], Dx[g][3]);
       *reinterpret_cast<int4 *>(R + 2 * len + o) = make_int4(iv[0], iv[1], iv[2], iv[3]);
@@ -1479,8 +1490,35 @@ __device__ __forceinline__ void dp_row_striped(int lane, int start, int len, int
   }
 }
 
-// Dispatches one int32 row to the striped tile of the right width.
+// A band wider than one tile (up to RING_WIDE_LEN): 512-column segments
+// chained by their insertion carry, then the row into the ring (each lane
+// copies the columns it wrote).
 template <bool ADAPT>
+__device__ __forceinline__ void dp_row_wide(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
+                                            const int32_t *mrow, int32_t E, int32_t O, unsigned vmask, int ps,
+                                            int pl, int pos, const int32_t *g, int32_t *rm, int32_t *rd, int cap,
+                                            int pos_i, int32_t &bv, int &bj) {
+  int32_t carry = NEG32;
+  int c0 = 0;
+  for (; c0 + RING_MAX_LEN < len; c0 += RING_MAX_LEN)
+    dp_row_striped<4, ADAPT, true>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i,
+                                   bv, bj, c0, &carry);
+  if (len - c0 <= 256)  // the last segment: two stripes when they cover it
+    dp_row_striped<2, ADAPT, true>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i,
+                                   bv, bj, c0, &carry);
+  else
+    dp_row_striped<4, ADAPT, true>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i,
+                                   bv, bj, c0, &carry);
+  __syncwarp();
+  for (int o = 4 * lane; o < len; o += 128) {
+    const int x = ring_at(pos_i, start, start + o, cap);
+    *reinterpret_cast<int4 *>(rm + x) = *reinterpret_cast<const int4 *>(R + o);
+    *reinterpret_cast<int4 *>(rd + x) = *reinterpret_cast<const int4 *>(R + len + o);
+  }
+}
+
+// Dispatches one int32 row to the striped tile of the right width.
+template <bool ADAPT, bool WIDE = false>
 __device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_t *R, const uint8_t *seq8,
                                             const int32_t *mrow, int32_t E, int32_t O, unsigned vmask, int ps,
                                             int pl, int pos, const int32_t *g, int32_t *rm, int32_t *rd, int cap,
@@ -1491,8 +1529,10 @@ __device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_
     dp_row_striped<2, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
   else if (len <= 384)
     dp_row_striped<3, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
-  else
+  else if (!WIDE || len <= RING_MAX_LEN)
     dp_row_striped<4, ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
+  else if constexpr (WIDE)
+    dp_row_wide<ADAPT>(lane, start, len, R, seq8, mrow, E, O, vmask, ps, pl, pos, g, rm, rd, cap, pos_i, bv, bj);
 }
 
 // ---------------------------------------------------------------------------
@@ -1643,9 +1683,9 @@ __device__ __forceinline__ int ring_pos(int64_t po, int64_t off, int64_t ring_fl
 // Copies row 0 (arena offset 0, computed serially) into the ring; returns the
 // ring floor (1 when the row is too wide to enter it).
 template <typename S>
-__device__ inline int64_t ring_put_row0(int32_t *rm, int32_t *rd, const S *A, int len) {
+__device__ inline int64_t ring_put_row0(int32_t *rm, int32_t *rd, const S *A, int len, int row_max) {
   const int lane = threadIdx.x & 31;
-  if (len > RING_MAX_LEN) return 1;
+  if (len > row_max) return 1;
   for (int c = lane; c < len; c += 32) {
     rm[c] = int32_t(A[c]);
     rd[c] = int32_t(A[len + c]);
@@ -1655,7 +1695,7 @@ __device__ inline int64_t ring_put_row0(int32_t *rm, int32_t *rd, const S *A, in
 }
 
 // One row by the generic interleaved loop (int64 kernel, rows wider than
-// RING_MAX_LEN, or more than 32 predecessors): 32-column chunks, predecessor rows
+// the kernel's ring row limit, or more than 32 predecessors): 32-column chunks, predecessor rows
 // from the arena, a warp-shuffle scan per chunk with a serial carry.
 template <typename S>
 __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *R, const S *A, const Scratch &s,
@@ -2066,10 +2106,10 @@ __device__ uint32_t dp_wave(const Scratch &s, int n, int32_t *A, const uint8_t *
 // the arena as (-1 - cum_hi, band start, band length, cum_lo) with cum the
 // predecessor's cumulative band length (its arena offset is 3 x cum); an
 // entry whose predecessor is skipped has band length 0. A row goes through
-// the ring when `ring` is set, its band is at most RING_MAX_LEN and it has at
+// the ring when `ring` is set, its band is at most row_max and it has at
 // most 32 predecessors (row 0: when its band fits). Counts the row kinds and
 // the predecessors read from the arena into `w`.
-__device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w) {
+__device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w, int row_max) {
   const int lane = threadIdx.x & 31;
   int carry = 0;  // rows before this block that did not go through the ring
   uint64_t g4 = 0, gen = 0, far = 0;
@@ -2078,7 +2118,7 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w)
     bool fast = true;
     if (i < n) {
       const int len = s.row_len[i], pc = s.pred_cnt[i];
-      fast = ring && len <= RING_MAX_LEN && (i == 0 || pc <= 32);
+      fast = ring && len <= row_max && (i == 0 || pc <= 32);
       if (i > 0 && len > 0) {
         g4 += fast && len > 384 ? 1 : 0;
         gen += fast ? 0 : 1;
@@ -2103,7 +2143,7 @@ __device__ inline void plan_rows(Scratch &s, int n, bool ring, int cap, Work *w)
         } else {
           const uint64_t cum = uint64_t(po / 3);
           e = make_int4(-1 - int(cum >> 31), m.y, m.z, int(cum & 0x7fffffffu));
-          if (s.row_len[i] > 0 && s.row_len[i] <= RING_MAX_LEN) ++far;
+          if (s.row_len[i] > 0 && s.row_len[i] <= row_max) ++far;
         }
       }
       s.pent[pb + t] = e;
@@ -2163,11 +2203,16 @@ __device__ inline void fill_pmeta(Scratch &s, int n) {
 
 // One DP kernel invocation (poa_simd_arena, align.rs:588-911, or
 // poa_scalar_i64, align.rs:913-1162) by a whole warp.
-template <typename S>
+// WIDE: bands up to RING_WIDE_LEN columns go through the striped tiles (in
+// 512-column segments); otherwise bands above RING_MAX_LEN take the generic
+// row. The batched kernel keeps the narrower form (its register budget), the
+// seed-window kernels, whose bands are up to twice the window band, the wide.
+template <typename S, bool WIDE = false>
 __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t arena_bytes, int beg_id, int end_id,
                               const uint8_t *query, int qlen, bool adaptive_arg, uint64_t band_b, uint64_t f,
                               Scratch &s, int *n_items, Work *cells, WarpSmem *sm) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
+  constexpr int kRowMax = WIDE ? RING_WIDE_LEN : RING_MAX_LEN;
   const int lane = threadIdx.x & 31;
   if (beg_id >= J->n_nodes || end_id >= J->n_nodes) return ST_ANCHOR_NOT_IN_GRAPH;
   const int beg = J->rank[beg_id], end = J->rank[end_id];
@@ -2337,11 +2382,11 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         return st;
       }
     }
-    plan_rows(s, n, ring, rcap, cells);
+    plan_rows(s, n, ring, rcap, cells, kRowMax);
     cells->pred_cells += pred_overlap_cells(s, n);
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
     __syncwarp();
-    if (ring) ring_put_row0(rm, rd, A, s.row_len[0]);
+    if (ring) ring_put_row0(rm, rd, A, s.row_len[0], kRowMax);
     // a lone giant's block-mates join the row loop (cooperative rows)
     const bool coop = ring && sm->rv.pad[0] != 0;
     CoopDesc *cd = coop ? reinterpret_cast<CoopDesc *>(sm->ring_m) : nullptr;
@@ -2406,13 +2451,13 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         }
       }
       S *R = A + off;
-      if (ring && len <= RING_MAX_LEN && pc <= 32) {
+      if (ring && len <= kRowMax && pc <= 32) {
         const bool ok = mt.z > 0;
         const int64_t mcum = mt.x < 0 ? ((int64_t(-1 - mt.x) << 31) | int64_t(uint32_t(mt.w))) : 0;
         const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + 3 * mcum;
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
-        if (coop) {
+        if (coop && len <= RING_MAX_LEN) {
           const int slot = __popc(vmask & ((1u << lane) - 1u));
           if (ok) {
             cd->ps[slot] = mt.y;
@@ -2435,7 +2480,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         }
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
-        dp_row_fast<false>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
+        dp_row_fast<false, WIDE>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
                            mt.y, mt.z, (ok && mt.x >= 0) ? mt.x : -1, my_g, rm, rd, rcap, pos_i, bv, bj);
         __syncwarp();
         continue;
@@ -2495,7 +2540,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         }
         if (lane == 0) dp_row0<S>(R, len, s00, E, O);
         __syncwarp();
-        if (kFastType && sm) ring_floor = ring_put_row0(rm, rd, A, len);
+        if (kFastType && sm) ring_floor = ring_put_row0(rm, rd, A, len, kRowMax);
         continue;
       }
       const int node = J->rank_to_node[beg + i];
@@ -2503,7 +2548,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
       const int pb = s.pred_start[i], pc = s.pred_cnt[i];
       S bestv = ScoreTraits<S>::LOWEST;
       int bestj = INT32_MAX;
-      if (kFastType && sm && len <= RING_MAX_LEN && pc <= 32) {
+      if (kFastType && sm && len <= kRowMax && pc <= 32) {
         if (len > 384) cells->rows_g4 += 1;
         int my_ps = 0, my_pl = 0, my_pos = -1;
         const int32_t *my_g = nullptr;
@@ -2524,7 +2569,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
         int32_t bv = INT32_MIN;
         int bj = INT32_MAX;
-        dp_row_fast<true>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
+        dp_row_fast<true, WIDE>(lane, start, len, reinterpret_cast<int32_t *>(R), q8, mrow, int32_t(E), int32_t(O), vmask,
                           my_ps, my_pl, my_pos, my_g, rm, rd, rcap, int((off / 3) % rcap), bv, bj);
         bestv = S(bv);
         bestj = bj;
@@ -2564,25 +2609,28 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
 }
 
 // poa_inner (align.rs:531-545): score-guard dispatch.
+template <bool WIDE = false>
 __device__ inline int32_t poa_inner(Job *J, const DevParams &P, char *arena, int64_t bytes, int beg_id, int end_id,
                                     const uint8_t *q, int qlen, bool adaptive, uint64_t band_b, uint64_t f,
                                     Scratch &s, int *n_items, Work *cells, WarpSmem *sm) {
   const bool use32 = P.kernel == 1 || (P.kernel == 0 && i32_scores_safe(J, P, beg_id, end_id, qlen));
   if (use32)
-    return poa_kernel<int32_t>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells,
+    return poa_kernel<int32_t, WIDE>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells,
                                sm);
-  return poa_kernel<int64_t>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells,
+  return poa_kernel<int64_t, WIDE>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, f, s, n_items, cells,
                              sm);
 }
 
 // poa (align.rs:192-211): on an alignment error with f != 0, retry with the
 // full matrix (f = 0, static band).
+template <bool WIDE = false>
 __device__ inline int32_t poa_retry(Job *J, const DevParams &P, char *arena, int64_t bytes, int beg_id, int end_id,
                                     const uint8_t *q, int qlen, bool adaptive, uint64_t band_b, Scratch &s,
                                     int *n_items, Work *cells, WarpSmem *sm) {
-  int32_t st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, P.f, s, n_items, cells, sm);
+  int32_t st =
+      poa_inner<WIDE>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive, band_b, P.f, s, n_items, cells, sm);
   if (is_alignment_error(st) && P.f != 0)
-    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, false, band_b, 0, s, n_items, cells, sm);
+    st = poa_inner<WIDE>(J, P, arena, bytes, beg_id, end_id, q, qlen, false, band_b, 0, s, n_items, cells, sm);
   return st;
 }
 

@@ -188,6 +188,8 @@ struct poa_ctx {
   size_t qbuf_bytes = 0;
   char *dlbuf = nullptr;  // graph downloads: packed records (grow-only, reused)
   size_t dlbuf_bytes = 0;
+  int32_t *h_dl = nullptr;  // pinned host copy of the last graph download
+  size_t h_dl_bytes = 0;
   int4 *items = nullptr;
   int32_t *n_items = nullptr;
   size_t items_cap = 0;
@@ -234,13 +236,26 @@ struct poa_ctx {
     qbuf = (uint8_t *)dalloc(bytes);
     qbuf_bytes = bytes;
   }
+  // Graphs grow read by read: both download buffers grow by half again so
+  // that a growing graph re-allocates them O(log n) times.
   void ensure_dlbuf(size_t bytes) {
     if (dlbuf_bytes >= bytes) return;
+    size_t want = std::max(bytes, dlbuf_bytes + dlbuf_bytes / 2);
     dfree(dlbuf, dlbuf_bytes);
     dlbuf = nullptr;
     dlbuf_bytes = 0;
-    dlbuf = (char *)dalloc(bytes);
-    dlbuf_bytes = bytes;
+    if (allocated + want > budget) want = bytes;
+    dlbuf = (char *)dalloc(want);
+    dlbuf_bytes = want;
+  }
+  void ensure_h_dl(size_t bytes) {
+    if (h_dl_bytes >= bytes) return;
+    if (h_dl) cudaFreeHost(h_dl);
+    h_dl = nullptr;
+    const size_t grown = std::max(bytes, h_dl_bytes + h_dl_bytes / 2);
+    h_dl_bytes = 0;
+    CK(cudaHostAlloc(reinterpret_cast<void **>(&h_dl), grown, cudaHostAllocDefault));
+    h_dl_bytes = grown;
   }
   void ensure_items(size_t n) {
     if (items_cap >= n) return;
@@ -385,16 +400,16 @@ struct poa_graph {
     const int64_t words = packed_words(h, sigma);
     // the context's download buffer (grown, never freed per call: a
     // cudaFree would synchronise the device on every download)
-    ctx->ensure_dlbuf(size_t(words) * 4 + 256);
-    int64_t *d_off = reinterpret_cast<int64_t *>(ctx->dlbuf);
-    int32_t *d_id = reinterpret_cast<int32_t *>(ctx->dlbuf + 16);
-    int32_t *d_out = reinterpret_cast<int32_t *>(ctx->dlbuf + 256);
-    std::vector<int32_t> rec(static_cast<size_t>(words));
-    CK(cudaMemsetAsync(ctx->dlbuf, 0, 32, ctx->stream));  // offset 0, id 0
-    CK(launch_pack(d_job, d_id, 1, d_off, d_out, sigma, ctx->stream));
-    CK(cudaMemcpyAsync(rec.data(), d_out, size_t(words) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    // layout: per-block entry counts of the packing kernels, then the record
+    constexpr size_t kRecAt = size_t(kPackOneMaxBlocks) * 16 + 256;
+    ctx->ensure_dlbuf(size_t(words) * 4 + kRecAt);
+    ctx->ensure_h_dl(size_t(words) * 4);
+    int64_t *d_part = reinterpret_cast<int64_t *>(ctx->dlbuf);
+    int32_t *d_out = reinterpret_cast<int32_t *>(ctx->dlbuf + kRecAt);
+    CK(launch_pack_one(d_job, h.n_nodes, d_part, d_out, sigma, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_dl, d_out, size_t(words) * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    return HostGraph::parse(rec.data());
+    return HostGraph::parse(ctx->h_dl);
   }
 };
 
@@ -1190,6 +1205,7 @@ void poa_ctx_destroy(poa_ctx *ctx) {
   ctx->dfree(ctx->arena, size_t(ctx->arena_bytes));
   ctx->dfree(ctx->qbuf, ctx->qbuf_bytes);
   ctx->dfree(ctx->dlbuf, ctx->dlbuf_bytes);
+  if (ctx->h_dl) cudaFreeHost(ctx->h_dl);
   ctx->dfree(ctx->items, 0);
   ctx->dfree(ctx->d_matrix, 0);
   ctx->dfree(ctx->d_encode, 0);

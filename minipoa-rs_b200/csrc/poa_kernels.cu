@@ -316,10 +316,10 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
   if (mode == 0) {
     st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, warp_smem());
   } else if (retry) {
-    st = poa_retry(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, s, &n_items, &cells,
+    st = poa_retry<true>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, s, &n_items, &cells,
                    warp_smem());
   } else {
-    st = poa_inner(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, P.f, s, &n_items, &cells,
+    st = poa_inner<true>(J, P, arena, bytes, beg_id, end_id, q, qlen, adaptive != 0, band_b, P.f, s, &n_items, &cells,
                    warp_smem());
   }
   if (st == ST_OK)
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   Scratch s;
   int n_items = 0;
   Work cells{};
-  const int32_t st = poa_retry(J, P, arenas + w * slot_bytes, slot_bytes, d.x, d.y, query + d.z, qlen, adaptive,
+  const int32_t st = poa_retry<true>(J, P, arenas + w * slot_bytes, slot_bytes, d.x, d.y, query + d.z, qlen, adaptive,
                                band[w], s, &n_items, &cells, warp_smem());
   if (st == ST_OK)
     for (int k = lane; k < n_items; k += 32) items[item_off[w] + k] = s.items[k];
