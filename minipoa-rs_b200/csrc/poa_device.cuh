@@ -70,6 +70,7 @@ struct DevParams {
   int32_t row_wave;       // static-band int32 rows: 0 one at a time, 1 wavefront where suited, 2 wavefront
   int32_t byte_prof;      // sigma <= 8 and every score fits a signed byte (dp_wave's packed profile)
   int32_t giant_alone;    // batched runs: a giant's block keeps only the giant and its helpers
+  int32_t wide_rows;      // batched runs: the kernel form with bands up to 2048 columns in striped segments
   uint64_t b, f;
   uint64_t largest;       // max(|matrix|, |O|, |E|) of i32_scores_safe
 };
@@ -2635,6 +2636,7 @@ __device__ inline int32_t poa_retry(Job *J, const DevParams &P, char *arena, int
 }
 
 // align::align (align.rs:81-98) for unseeded parameters; writes s.items.
+template <bool WIDE = false>
 __device__ inline int32_t align_query(Job *J, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q,
                                       int qlen, Scratch &s, int *n_items, Work *cells, WarpSmem *sm) {
   const int lane = threadIdx.x & 31;
@@ -2648,7 +2650,7 @@ __device__ inline int32_t align_query(Job *J, const DevParams &P, char *arena, i
     return ST_OK;
   }
   if (P.seeding) return ST_SEEDING_UNSUPPORTED;
-  return poa_retry(J, P, arena, bytes, 0, 1, q, qlen, P.adaptive != 0, P.b, s, n_items, cells, sm);
+  return poa_retry<WIDE>(J, P, arena, bytes, 0, 1, q, qlen, P.adaptive != 0, P.b, s, n_items, cells, sm);
 }
 
 // Re-sorts the rank windows of reorder_incremental (warp-wide). spans[k] =
@@ -2875,6 +2877,7 @@ __device__ inline int32_t finalize_order(Job *J, char *arena, int64_t bytes) {
 
 // One step of extend_graph (lib.rs:199-201): align, add_path, toposort(false).
 // Capacity is checked before the DP so a full graph stops cleanly.
+template <bool WIDE = false>
 __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, int64_t bytes, const uint8_t *q,
                                      int qlen, int r, WarpSmem *sm) {
   const int lane = threadIdx.x & 31;
@@ -2888,7 +2891,7 @@ __device__ inline int32_t extend_one(Job *J, const DevParams &P, char *arena, in
   Scratch s;
   int n_items = 0;
   Work cells{};
-  int32_t st = align_query(J, P, arena, bytes, q, qlen, s, &n_items, &cells, sm);
+  int32_t st = align_query<WIDE>(J, P, arena, bytes, q, qlen, s, &n_items, &cells, sm);
   if (st != ST_OK) return st;
   const uint64_t t_u0 = phase_clock();
   const int n_old = J->n_nodes;

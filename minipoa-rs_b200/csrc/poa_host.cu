@@ -302,6 +302,14 @@ struct poa_ctx {
     P.row_wave = 0;
     if (rows_env && std::strcmp(rows_env, "auto") == 0) P.row_wave = 1;
     if (rows_env && std::strcmp(rows_env, "wave") == 0) P.row_wave = 2;
+    // batched kernel form: bands up to 2048 columns as striped segments
+    // (MINIPOA_WIDE_ROWS=1, or by default with the full matrix, f = 0, whose
+    // bands are not bounded by the read length) or the form that keeps
+    // rows above 512 columns on the generic row (=0)
+    const char *wide_env = std::getenv("MINIPOA_WIDE_ROWS");
+    P.wide_rows = hp.f == 0 ? 1 : 0;
+    if (wide_env && std::strcmp(wide_env, "1") == 0) P.wide_rows = 1;
+    if (wide_env && std::strcmp(wide_env, "0") == 0) P.wide_rows = 0;
     P.byte_prof = P.sigma <= 8 ? 1 : 0;
     for (int32_t v : hp.matrix)
       if (v < -128 || v > 127) P.byte_prof = 0;

@@ -57,22 +57,30 @@ def _full_machine_sets(seed, n_giants, giant_len, giant_depth, n_small):
 
 
 @contextlib.contextmanager
-def _dp_rows(mode):
-    """Sets the static-band DP form of batches created inside the block:
-    "rows" (row at a time), "wave" (row wavefront), "auto" (each read's
-    choice) or None (the default)."""
-    old = os.environ.get("MINIPOA_DP_ROWS")
-    if mode is None:
-        os.environ.pop("MINIPOA_DP_ROWS", None)
+def _env(name, value):
+    old = os.environ.get(name)
+    if value is None:
+        os.environ.pop(name, None)
     else:
-        os.environ["MINIPOA_DP_ROWS"] = mode
+        os.environ[name] = value
     try:
         yield
     finally:
         if old is None:
-            os.environ.pop("MINIPOA_DP_ROWS", None)
+            os.environ.pop(name, None)
         else:
-            os.environ["MINIPOA_DP_ROWS"] = old
+            os.environ[name] = old
+
+
+@contextlib.contextmanager
+def _dp_rows(mode, wide=None):
+    """Sets the static-band DP form of batches created inside the block:
+    "rows" (row at a time), "wave" (row wavefront), "auto" (each read's
+    choice) or None (the default); and the batched kernel's row form: wide
+    "1" (bands up to 2048 columns in striped segments), "0" (the narrow
+    form) or None (the default for the parameters)."""
+    with _env("MINIPOA_DP_ROWS", mode), _env("MINIPOA_WIDE_ROWS", wide):
+        yield
 
 
 def _gfa_hashes_match(oracle, batch, params, sets):
@@ -81,11 +89,12 @@ def _gfa_hashes_match(oracle, batch, params, sets):
     return bad
 
 
-@pytest.mark.parametrize("adaptive,dp", [(False, "rows"), (False, "wave"), (False, "auto"), (True, None)])
-def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive, dp):
+@pytest.mark.parametrize("adaptive,dp,wide", [(False, "rows", None), (False, "wave", None), (False, "auto", None),
+                                             (True, None, None), (False, "rows", "1"), (True, None, "1")])
+def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive, dp, wide):
     params = Params(adaptive=adaptive)
     sets = _full_machine_sets(2024 + int(adaptive), 4, 4200, 30, 1180)
-    with _dp_rows(dp):
+    with _dp_rows(dp, wide):
         batch = mp.Batch(params, sets)
     batch.tune(8)  # full 8-warp blocks: the giant runs on warp 4 with warps 0-2 as helpers
     st = batch.run(0)
@@ -96,7 +105,11 @@ def test_full_machine_batch_with_giants_matches_oracle(mp, oracle, adaptive, dp)
 
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     assert st.slots == min(len(sets), sms * 8)
-    assert st.far_preds > 0, "no predecessor state was read back from the arena"
+    if wide is None:
+        # (the wide form keeps every row of these sets in the ring: its
+        # predecessors leave the ring only by distance, which these graphs'
+        # edges rarely reach; the wide-band tests cover its arena reads)
+        assert st.far_preds > 0, "no predecessor state was read back from the arena"
     if adaptive or dp == "rows":
         assert st.wave_reads == 0
         assert st.rows_g4 > 0, "no 4-stripe rows ran"
@@ -155,12 +168,16 @@ def test_protein_families_full_dp_wide_rows_match_oracle(mp, oracle):
                     s.append(int(rng.integers(0, 20)))  # insertion
             fam.append(bytes(alpha[x] for x in s))
         fams.append(fam)
-    for dp in ("rows", "wave"):
-        with _dp_rows(dp):
+    for dp, wide in (("rows", None), ("rows", "0"), ("wave", None)):
+        with _dp_rows(dp, wide):
             batch = mp.Batch(params, fams)
         st = batch.run(0)
-        if dp == "rows":
+        if dp == "rows" and wide == "0":
             assert st.rows_generic > 0, "no generic (wide) rows ran"
+        elif dp == "rows":
+            # -f0 selects the wide kernel form: rows of 600-800 columns in
+            # striped segments, none on the generic row
+            assert st.rows_g4 > 0 and st.rows_generic < st.rows_g4, (st.rows_g4, st.rows_generic)
         else:
             assert st.wave_reads > 0, "the row wavefront did not run"
         for f, reads in enumerate(fams):
