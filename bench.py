@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="length of the serving run at 80%% load")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: tune the batch's launch settings before the timed steps (0: defaults)")
+    ap.add_argument("--c4a-only", type=int, default=0,
+                    help="run only the protein-family configuration with this many families and print its "
+                         "key (a small case for profiling the wide kernel form)")
     ap.add_argument("--c4b-reads", type=int, default=3,
                     help="reads per set of the int64 run (8 sets x 100 kbp, match 1000; 0: skip)")
     ap.add_argument("--seeded-reads", type=int, default=100,
@@ -568,6 +571,12 @@ def load_traffic():
 
 def main():
     args = parse()
+    if args.c4a_only:
+        import minipoa_b200 as mp
+
+        ctx = mp.Context(0, mem_budget=int(args.mem_budget_gb * (1 << 30)))
+        print(json.dumps({"c4a_protein": c4a_bench(mp, ctx, args.c4a_only)}))
+        return
     world, rank, local, pg = dist_setup(args)
     from minipoa_b200 import workloads
     from minipoa_b200.params import Params
