@@ -1696,57 +1696,105 @@ __device__ inline int64_t ring_put_row0(int32_t *rm, int32_t *rd, const S *A, in
 }
 
 // One row by the generic interleaved loop (int64 kernel, rows wider than
-// the kernel's ring row limit, or more than 32 predecessors): 32-column chunks, predecessor rows
-// from the arena, a warp-shuffle scan per chunk with a serial carry.
+// the kernel's ring row limit, or more than 32 predecessors): 32-column
+// chunks, predecessor rows from the arena, a warp-shuffle scan per chunk with
+// a serial carry. Two chunks are taken per step, so the predecessor loads of
+// both are in flight together (only the carry links them). With at most 32
+// predecessors, lane t holds predecessor t's band and arena row for the
+// whole row and the chunks take them by shuffle.
 template <typename S>
 __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *R, const S *A, const Scratch &s,
                                                int pb, int pc, const int32_t *mrow, S E, S O, bool adapt, S &bestv,
                                                int &bestj) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
   const int stop = start + len;
+  const bool held = pc <= 32;
+  int my_ps = 0, my_pl = 0;
+  const S *my_q = A;
+  if (held && lane < pc) {
+    const int p = s.pred[pb + lane].x;
+    if (p >= 0) {
+      my_ps = s.row_start[p];
+      my_pl = s.row_len[p];
+      my_q = A + s.row_off[p];
+    }
+  }
+  const unsigned vmask = __ballot_sync(FULL, my_pl > 0);
   S carry = NEGV;
-  for (int c0 = start; c0 < stop; c0 += 32) {
-    const int j = c0 + lane;
-    const bool valid = j < stop;
-    S M = NEGV, D = NEGV;
-    if (valid) {
+  for (int c0 = start; c0 < stop; c0 += 64) {
+    S M[2], D[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      M[h] = NEGV;
+      D[h] = NEGV;
+    }
+    if (held) {
+      unsigned vm = vmask;
+      while (vm) {
+        const int t = __ffs(vm) - 1;
+        vm &= vm - 1;
+        const int ps = __shfl_sync(FULL, my_ps, t), pl = __shfl_sync(FULL, my_pl, t);
+        const S *Q = reinterpret_cast<const S *>(__shfl_sync(FULL, (long long)my_q, t));
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = c0 + 32 * h + lane;
+          if (j < stop && j >= ps && j < ps + pl) {
+            const int k = j - ps;
+            const S mp = Q[k], dp = Q[pl + k];
+            const S dg = k > 0 ? Q[k - 1] : NEGV;
+            M[h] = maxs(M[h], dg);
+            D[h] = maxs(D[h], maxs<S>(dp + E, mp + O));
+          }
+        }
+      }
+    } else {
       for (int t = 0; t < pc; ++t) {
         const int p = s.pred[pb + t].x;
         if (p < 0) continue;
         const int ps = s.row_start[p], pl = s.row_len[p];
-        if (j >= ps && j < ps + pl) {
-          const S *Q = A + s.row_off[p];
-          const int k = j - ps;
-          const S mp = Q[k], dp = Q[pl + k];
-          const S dg = k > 0 ? Q[k - 1] : NEGV;
-          M = maxs(M, dg);
-          D = maxs(D, maxs<S>(dp + E, mp + O));
+        const S *Q = A + s.row_off[p];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = c0 + 32 * h + lane;
+          if (j < stop && j >= ps && j < ps + pl) {
+            const int k = j - ps;
+            const S mp = Q[k], dp = Q[pl + k];
+            const S dg = k > 0 ? Q[k - 1] : NEGV;
+            M[h] = maxs(M[h], dg);
+            D[h] = maxs(D[h], maxs<S>(dp + E, mp + O));
+          }
         }
       }
     }
-    const S prof = valid ? S(mrow[s.seq[j]]) : S(0);
-    const S md = maxs<S>(M + prof, D);
-    S x = md + O;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const S y = shfl_up_s(x, d);
-      if (lane >= d) x = maxs<S>(x, y + S(d) * E);
-    }
-    x = maxs<S>(x, carry + S(lane + 1) * E);
-    S I = shfl_up_s(x, 1);
-    if (lane == 0) I = carry;
-    const S Mf = maxs(md, I);
-    if (valid) {
-      const int c = j - start;
-      R[c] = Mf;
-      R[len + c] = D;
-      R[2 * len + c] = I;
-      if (adapt && Mf > bestv) {
-        bestv = Mf;
-        bestj = j;
+    for (int h = 0; h < 2; ++h) {
+      if (c0 + 32 * h >= stop) break;  // (warp-uniform)
+      const int j = c0 + 32 * h + lane;
+      const bool valid = j < stop;
+      const S prof = valid ? S(mrow[s.seq[j]]) : S(0);
+      const S md = maxs<S>(M[h] + prof, D[h]);
+      S x = md + O;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const S y = shfl_up_s(x, d);
+        if (lane >= d) x = maxs<S>(x, y + S(d) * E);
       }
+      x = maxs<S>(x, carry + S(lane + 1) * E);
+      S I = shfl_up_s(x, 1);
+      if (lane == 0) I = carry;
+      const S Mf = maxs(md, I);
+      if (valid) {
+        const int c = j - start;
+        R[c] = Mf;
+        R[len + c] = D[h];
+        R[2 * len + c] = I;
+        if (adapt && Mf > bestv) {
+          bestv = Mf;
+          bestj = j;
+        }
+      }
+      carry = shfl_s(x, 31);
     }
-    carry = shfl_s(x, 31);
   }
 }
 
