@@ -1698,8 +1698,9 @@ __device__ inline int64_t ring_put_row0(int32_t *rm, int32_t *rd, const S *A, in
 // One row by the generic interleaved loop (int64 kernel, rows wider than
 // the kernel's ring row limit, or more than 32 predecessors): 32-column
 // chunks, predecessor rows from the arena, a warp-shuffle scan per chunk with
-// a serial carry. Two chunks are taken per step, so the predecessor loads of
-// both are in flight together (only the carry links them). With at most 32
+// a serial carry. Several chunks are taken per step (two for int32, four for
+// int64, whose rows are the widest), so the predecessor loads and the scans
+// of all of them are in flight together (only the carry links them). With at most 32
 // predecessors, lane t holds predecessor t's band and arena row for the
 // whole row and the chunks take them by shuffle.
 template <typename S>
@@ -1707,6 +1708,7 @@ __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *
                                                int pb, int pc, const int32_t *mrow, S E, S O, bool adapt, S &bestv,
                                                int &bestj) {
   constexpr S NEGV = ScoreTraits<S>::NEGV;
+  constexpr int NCH = sizeof(S) == 8 ? 4 : 2;  // chunks per step
   const int stop = start + len;
   const bool held = pc <= 32;
   int my_ps = 0, my_pl = 0;
@@ -1721,10 +1723,10 @@ __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *
   }
   const unsigned vmask = __ballot_sync(FULL, my_pl > 0);
   S carry = NEGV;
-  for (int c0 = start; c0 < stop; c0 += 64) {
-    S M[2], D[2];
+  for (int c0 = start; c0 < stop; c0 += 32 * NCH) {
+    S M[NCH], D[NCH];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NCH; ++h) {
       M[h] = NEGV;
       D[h] = NEGV;
     }
@@ -1736,7 +1738,7 @@ __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *
         const int ps = __shfl_sync(FULL, my_ps, t), pl = __shfl_sync(FULL, my_pl, t);
         const S *Q = reinterpret_cast<const S *>(__shfl_sync(FULL, (long long)my_q, t));
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NCH; ++h) {
           const int j = c0 + 32 * h + lane;
           if (j < stop && j >= ps && j < ps + pl) {
             const int k = j - ps;
@@ -1754,7 +1756,7 @@ __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *
         const int ps = s.row_start[p], pl = s.row_len[p];
         const S *Q = A + s.row_off[p];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NCH; ++h) {
           const int j = c0 + 32 * h + lane;
           if (j < stop && j >= ps && j < ps + pl) {
             const int k = j - ps;
@@ -1767,7 +1769,7 @@ __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *
       }
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < NCH; ++h) {
       if (c0 + 32 * h >= stop) break;  // (warp-uniform)
       const int j = c0 + 32 * h + lane;
       const bool valid = j < stop;

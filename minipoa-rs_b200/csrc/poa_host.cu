@@ -1725,8 +1725,8 @@ int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
       double gf;
       int alone;
     };
-    const Cand cand[] = {{kDefaultBatchWarpsPerSm, 1.5, 0}, {6, 1.5, 1}, {4, 1.5, 0}, {5, 1.5, 0},
-                         {7, 1.5, 0},  {8, 1.5, 0},  {8, 1.5, 1}, {6, 3.0, 0}};
+    const Cand cand[] = {{kDefaultBatchWarpsPerSm, 1.5, 0}, {6, 1.5, 1}, {5, 1.5, 1}, {6, 1.0, 1}, {4, 1.5, 0},
+                         {5, 1.5, 0}, {7, 1.5, 0}, {8, 1.5, 0}, {8, 1.5, 1}};
     double best_ms = 0;
     Cand best{b->warps_per_sm, b->giant_factor, b->giant_alone};
     int tried = 0;

@@ -25,7 +25,7 @@ def test_autotune_caches_a_setting_and_keeps_the_bytes(tmp_path, monkeypatch):
     b.run(0)
     want = b.output_all(2)
     t = b.autotune()
-    assert t.trials == 8 and t.warps_per_sm in (4, 5, 6, 7, 8) and t.giant_factor in (1.5, 3.0)
+    assert t.trials == 9 and t.warps_per_sm in (4, 5, 6, 7, 8) and t.giant_factor in (1.0, 1.5)
     assert t.giant_alone in (0, 1)
     assert b.output_all(2) == want
     b.run(0)
