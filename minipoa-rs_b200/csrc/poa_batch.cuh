@@ -155,7 +155,8 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   // the grid is rounded up to whole blocks; warps past the last slot own no
   // arena (they leave after the block's start-up barrier)
   const bool active = warp < slots;
-  char *arena = arenas + warp * slot_bytes;
+  // (teams: one arena per block, the job's warp 0 uses it)
+  char *arena = arenas + (P.teams ? int64_t(blockIdx.x) : warp) * slot_bytes;
   WarpSmem *sm = warp_smem();
   int32_t *queue = sched;
   int32_t *sm_count = sched + 4;
@@ -172,7 +173,16 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   ring_default(sm);
   __syncthreads();
   int first = -1, first_giant = 0;
-  if (!serve && active && lane == 0 && sm_ok) {
+  if (P.teams) {
+    // team launch (a small batch): block b is job b's team, the job on warp
+    // 0 and the other three warps its helpers; no job comes from the queue
+    if (!serve && active && lane == 0 && (threadIdx.x >> 5) == 0 && blockIdx.x < unsigned(n_jobs)) {
+      first = int(blockIdx.x);
+      first_giant = 1;
+      atomicAdd(&block_giant, 1);
+      giant_warp = 0;
+    }
+  } else if (!serve && active && lane == 0 && sm_ok) {
     const int level = atomicAdd(&sm_count[smid], 1);
     if (level < SCHED_LEVELS) {
       const int64_t p0 = int64_t(level) * num_sms + atomicAdd(&level_count[level], 1);
@@ -270,6 +280,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     } else {
       int q = first;
       first = -1;
+      if (q < 0 && P.teams) break;  // a team runs its own job only
       if (q < 0) {
         if (lane == 0) {
           do {

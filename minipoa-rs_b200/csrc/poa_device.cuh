@@ -71,6 +71,7 @@ struct DevParams {
   int32_t byte_prof;      // sigma <= 8 and every score fits a signed byte (dp_wave's packed profile)
   int32_t giant_alone;    // batched runs: a giant's block keeps only the giant and its helpers
   int32_t wide_rows;      // batched runs: the kernel form with bands up to 2048 columns in striped segments
+  int32_t teams;          // batched runs: one 4-warp block per job (a job and its three helpers)
   uint64_t b, f;
   uint64_t largest;       // max(|matrix|, |O|, |E|) of i32_scores_safe
 };
@@ -1547,7 +1548,8 @@ __device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_
 // done. The arithmetic is the single-warp striped row's: the stripe carries
 // compose as carry[g+1] = max(aggregate[g], carry[g] + 128E).
 constexpr int COOP_ROWS = 0, COOP_DONE = 1;  // phase modes
-constexpr int COOP_ROW = 0, COOP_STOP = 1;   // row operations
+constexpr int COOP_GEN_MIN_LEN = 256;         // narrower int64 rows: the leader alone
+constexpr int COOP_ROW = 0, COOP_STOP = 1, COOP_GEN = 2;  // row operations
 struct CoopDesc {
   int mode, op, start, len, pos_i, n_pred, cap, pad0;
   int32_t E, O, pad1, pad2;
@@ -1558,8 +1560,19 @@ struct CoopDesc {
   int32_t agg[4];
   int ps[32], pl[32], pos[32];
   const int32_t *g[32];
+  // int64 rows (COOP_GEN): per read, the gaps, the arena and the plan arrays;
+  // per row, its arena row and predecessor list; per warp, its segment's
+  // insertion state leaving the segment
+  int64_t E64, O64;
+  const int64_t *gA;
+  const int32_t *grs, *grl, *gseq;
+  const int64_t *gro;
+  int64_t *gR;
+  const int2 *gpred;
+  int64_t agg64[4];
 };
 static_assert(sizeof(CoopDesc) <= sizeof(int32_t) * RING_CAP, "CoopDesc must fit a ring array");
+__device__ inline void coop_gen64(CoopDesc *c, int g);
 
 __device__ __forceinline__ void coop_bar(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 
@@ -1658,7 +1671,10 @@ __device__ inline void coop_helper(CoopDesc *c, int g) {
     for (;;) {
       coop_bar(1);
       if (c->op == COOP_STOP) break;
-      coop_stripe(c, g);
+      if (c->op == COOP_GEN)
+        coop_gen64(c, g);
+      else
+        coop_stripe(c, g);
     }
   }
 }
@@ -1798,6 +1814,108 @@ __device__ __forceinline__ void dp_row_generic(int lane, int start, int len, S *
       carry = shfl_s(x, 31);
     }
   }
+}
+
+// Cooperative int64 rows: a giant job's generic rows (at most 32
+// predecessors) computed by its warp and three helpers, warp g taking the g-th
+// quarter of the band (32-column aligned). Pass 1: each warp computes M and D
+// from the predecessors, md and its segment's insertion scan as if the
+// segment began the row (from a value below every state), storing md, D and
+// that scan; the segments' last scan values are published (barrier 1). Pass
+// 2: each warp composes the insertion state entering its segment from the
+// segments before it, carry = max(last[h], carry + E x width[h]) from the
+// row's initial NEGV, and finishes its columns: x = max(scan, carry + E x
+// distance), I = the x of the column before, M = max(md, I). Max-plus
+// addition distributes exactly over max in integers, so every stored state
+// equals the one-warp generic row's (barrier 1 again once the row is written).
+__device__ inline void coop_gen64(CoopDesc *c, int g) {
+  using S = int64_t;
+  constexpr S NEGV = NEG64;
+  constexpr S BELOW = -(S(1) << 61);
+  const int lane = threadIdx.x & 31;
+  const int start = c->start, len = c->len, stop = start + len;
+  const S E = c->E64, O = c->O64;
+  const int seg = (len + 127) / 128 * 32;
+  const int a = start + g * seg, b = min(stop, a + seg);
+  S *R = c->gR;
+  const S *A = c->gA;
+  const int32_t *mrow = c->mrow;
+  const int32_t *seq = c->gseq;
+  const int pc = c->n_pred;
+  int my_ps = 0, my_pl = 0;
+  const S *my_q = A;
+  if (lane < pc) {
+    const int p = c->gpred[lane].x;
+    if (p >= 0) {
+      my_ps = c->grs[p];
+      my_pl = c->grl[p];
+      my_q = A + c->gro[p];
+    }
+  }
+  const unsigned vmask = __ballot_sync(FULL, my_pl > 0);
+  S lc = BELOW;
+  for (int c0 = a; c0 < b; c0 += 32) {
+    const int j = c0 + lane;
+    const bool valid = j < stop;
+    S M = NEGV, D = NEGV;
+    unsigned vm = vmask;
+    while (vm) {
+      const int t = __ffs(vm) - 1;
+      vm &= vm - 1;
+      const int ps = __shfl_sync(FULL, my_ps, t), pl = __shfl_sync(FULL, my_pl, t);
+      const S *Q = reinterpret_cast<const S *>(__shfl_sync(FULL, (long long)my_q, t));
+      if (valid && j >= ps && j < ps + pl) {
+        const int k = j - ps;
+        const S mp = Q[k], dp = Q[pl + k];
+        const S dg = k > 0 ? Q[k - 1] : NEGV;
+        M = maxs(M, dg);
+        D = maxs(D, maxs<S>(dp + E, mp + O));
+      }
+    }
+    const S prof = valid ? S(mrow[seq[j]]) : S(0);
+    const S md = maxs<S>(M + prof, D);
+    S x = md + O;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const S y = shfl_up_s(x, d);
+      if (lane >= d) x = maxs<S>(x, y + S(d) * E);
+    }
+    x = maxs<S>(x, lc + S(lane + 1) * E);
+    if (valid) {
+      const int cc = j - start;
+      R[cc] = md;
+      R[len + cc] = D;
+      R[2 * len + cc] = x;
+    }
+    lc = shfl_s(x, 31);
+  }
+  if (lane == 0) c->agg64[g] = lc;
+  coop_bar(1);
+  S cin = NEGV;
+  for (int h = 0; h < g; ++h) {
+    const int ah = start + h * seg, bh = min(stop, ah + seg);
+    if (bh > ah) cin = maxs<S>(c->agg64[h], cin + S(bh - ah) * E);
+  }
+  S prev = cin;  // x of the column before the chunk
+  for (int c0 = a; c0 < b; c0 += 32) {
+    const int j = c0 + lane;
+    const bool valid = j < stop;
+    const int cc = j - start;
+    S xt = BELOW, md = NEGV;
+    if (valid) {
+      xt = R[2 * len + cc];
+      md = R[cc];
+    }
+    xt = maxs<S>(xt, cin + S(j - a + 1) * E);
+    S I = shfl_up_s(xt, 1);
+    if (lane == 0) I = prev;
+    if (valid) {
+      R[cc] = maxs(md, I);
+      R[2 * len + cc] = I;
+    }
+    prev = shfl_s(xt, 31);
+  }
+  coop_bar(1);
 }
 
 // Row 0 (align.rs:737-750), serial on lane 0.
@@ -2438,8 +2556,9 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
     if (s.row_len[0] > 0 && lane == 0) dp_row0<S>(A + s.row_off[0], s.row_len[0], s00, E, O);
     __syncwarp();
     if (ring) ring_put_row0(rm, rd, A, s.row_len[0], kRowMax);
-    // a lone giant's block-mates join the row loop (cooperative rows)
-    const bool coop = ring && sm->rv.pad[0] != 0;
+    // a lone giant's block-mates join the row loop (cooperative rows: the
+    // striped int32 rows, or the int64 kernel's generic rows)
+    const bool coop = sm && sm->rv.pad[0] != 0 && (ring || !kFastType);
     CoopDesc *cd = coop ? reinterpret_cast<CoopDesc *>(sm->ring_m) : nullptr;
     if (coop) cells->coop = 1;
     if (coop) {
@@ -2451,6 +2570,13 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         cd->rm = rm;
         cd->rd = rd;
         cd->cap = rcap;
+        cd->E64 = int64_t(E);
+        cd->O64 = int64_t(O);
+        cd->gA = reinterpret_cast<const int64_t *>(A);
+        cd->grs = s.row_start;
+        cd->grl = s.row_len;
+        cd->gseq = s.seq;
+        cd->gro = s.row_off;
       }
       coop_bar(2);
     }
@@ -2535,6 +2661,22 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
                            mt.y, mt.z, (ok && mt.x >= 0) ? mt.x : -1, my_g, rm, rd, rcap, pos_i, bv, bj);
         __syncwarp();
         continue;
+      }
+      if constexpr (!kFastType) {
+        if (coop && pc <= 32 && len >= COOP_GEN_MIN_LEN) {
+          if (lane == 0) {
+            cd->op = COOP_GEN;
+            cd->start = start;
+            cd->len = len;
+            cd->n_pred = pc;
+            cd->gR = reinterpret_cast<int64_t *>(R);
+            cd->gpred = s.pred + pb;
+            cd->mrow = P.matrix + base * P.sigma;
+          }
+          coop_bar(1);
+          coop_gen64(cd, 0);  // the leader computes the first quarter
+          continue;
+        }
       }
       S bv = ScoreTraits<S>::LOWEST;
       int bj = INT32_MAX;

@@ -1005,6 +1005,7 @@ struct poa_batch {
   cudaGraphExec_t gexec = nullptr;
   int64_t g_slots = -1, g_slot_bytes = -1;
   int g_alone = -1;
+  int g_team = -1;
   int graph_launches = 0;
 
   // d_order holds two orders: the running pass's, and at base_order() the
@@ -1808,7 +1809,15 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
       int64_t slots = int64_t(sms) * wps;
       for (;;) {
         slots = std::max<int64_t>(1, std::min<int64_t>(slots, int64_t(pending.size())));
-        int64_t slot_bytes = b->arena_pool / slots / 256 * 256;
+        // a small batch (at most one set per two SMs) runs as teams: one
+        // 4-warp block per set, the set on warp 0 with three helper warps
+        // for its DP rows, one arena per block (not with the row wavefront
+        // forced: a warp leading helpers runs rows one at a time)
+        const bool team = passes == 0 && b->giant_factor > 0 && int64_t(pending.size()) * 2 <= sms &&
+                          b->P.row_wave != 2;
+        if (team) slots = 4 * int64_t(pending.size());
+        b->P.teams = team ? 1 : 0;
+        int64_t slot_bytes = b->arena_pool / (team ? slots / 4 : slots) / 256 * 256;
         if (b->slot_bytes_override && passes == 0)
           slot_bytes = std::min<int64_t>(int64_t(b->slot_bytes_override), slot_bytes);
         if (passes == 0) {
@@ -1816,7 +1825,8 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
           // the first pass as one CUDA graph (reset of every graph, queue
           // set-up, the persistent kernel), captured once per launch shape
           b->P.giant_alone = b->giant_alone;
-          if (!b->gexec || b->g_slots != slots || b->g_slot_bytes != slot_bytes || b->g_alone != b->giant_alone) {
+          if (!b->gexec || b->g_slots != slots || b->g_slot_bytes != slot_bytes || b->g_alone != b->giant_alone ||
+              b->g_team != int(team)) {
             if (b->gexec) cudaGraphExecDestroy(b->gexec);
             b->gexec = nullptr;
             CK(prepare_batch_kernel());
@@ -1839,6 +1849,7 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
             b->g_slots = slots;
             b->g_slot_bytes = slot_bytes;
             b->g_alone = b->giant_alone;
+            b->g_team = int(team);
           }
           // timing events stay outside the graph: an event recorded during
           // capture becomes a dependency marker, not a timestamp

@@ -182,6 +182,7 @@ cudaError_t launch_batch(const Job *jobs_dev, const int32_t *order, int n_jobs, 
   // spread over all SMs instead of filling a few
   int wpb = WARPS_PER_BLOCK;
   if (num_sms > 0 && slots < num_sms * WARPS_PER_BLOCK) wpb = std::max(1, (slots + num_sms - 1) / num_sms);
+  if (P.teams) wpb = 4;  // one block per job: the job and its three helpers
   const int blocks = (slots + wpb - 1) / wpb;
   const cudaError_t pe = prepare_batch_kernel();
   if (pe != cudaSuccess) return pe;
