@@ -1809,12 +1809,12 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
       int64_t slots = int64_t(sms) * wps;
       for (;;) {
         slots = std::max<int64_t>(1, std::min<int64_t>(slots, int64_t(pending.size())));
-        // a small batch (at most one set per two SMs) runs as teams: one
-        // 4-warp block per set, the set on warp 0 with three helper warps
-        // for its DP rows, one arena per block (not with the row wavefront
-        // forced: a warp leading helpers runs rows one at a time)
-        const bool team = passes == 0 && b->giant_factor > 0 && int64_t(pending.size()) * 2 <= sms &&
-                          b->P.row_wave != 2;
+        // a small batch (at most one set per SM) runs as teams: one 4-warp
+        // block per set, the set on warp 0 with three helper warps for its
+        // DP rows, one arena per block (not with the row wavefront forced: a
+        // warp leading helpers runs rows one at a time)
+        const bool team =
+            passes == 0 && b->giant_factor > 0 && int64_t(pending.size()) <= sms && b->P.row_wave != 2;
         if (team) slots = 4 * int64_t(pending.size());
         b->P.teams = team ? 1 : 0;
         int64_t slot_bytes = b->arena_pool / (team ? slots / 4 : slots) / 256 * 256;

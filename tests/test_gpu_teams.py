@@ -1,4 +1,4 @@
-"""Small batches (at most one read set per two SMs) run as teams: one 4-warp
+"""Small batches (at most one read set per SM) run as teams: one 4-warp
 block per set, the set on warp 0 and three helper warps on its DP rows. The
 int32 rows are split by stripes, the int64 kernel's generic rows by quarters
 of the band with the insertion state composed across them; graphs, ranks and
