@@ -8,6 +8,8 @@ import ctypes
 import dataclasses
 from typing import List, Optional, Sequence as Seq, Tuple
 
+import numpy as np
+
 from . import _lib
 from .params import AlignedBase, Params, Sequence
 
@@ -40,12 +42,24 @@ def _bytes(x) -> bytes:
 
 
 def _seq_arrays(seqs: Seq[bytes]):
+    """The C ABI's (pointer array, length array) for `seqs`: the sequences
+    joined into one buffer, each pointer its start in it (one copy of the
+    bytes, no per-sequence objects). The third value keeps the buffers alive
+    while the pointers are in use."""
     seqs = [_bytes(s) for s in seqs]
-    bufs = [(ctypes.c_uint8 * max(1, len(s))).from_buffer_copy(s if s else b"\0") for s in seqs]
-    arr = (ctypes.POINTER(ctypes.c_uint8) * max(1, len(seqs)))(
-        *[ctypes.cast(b, ctypes.POINTER(ctypes.c_uint8)) for b in bufs])
-    lens = (ctypes.c_int64 * max(1, len(seqs)))(*[len(s) for s in seqs])
-    return arr, lens, bufs
+    n = len(seqs)
+    lens = np.fromiter((len(s) for s in seqs), dtype=np.int64, count=n)
+    if n == 0:
+        lens = np.zeros(1, dtype=np.int64)
+    joined = b"".join(seqs) + b"\0"
+    base = np.frombuffer(joined, dtype=np.uint8)
+    starts = np.zeros(max(1, n), dtype=np.uint64)
+    if n > 1:
+        np.cumsum(lens[:-1], out=starts[1:].view(np.int64))
+    ptrs = starts + np.uint64(base.ctypes.data)
+    arr = ptrs.ctypes.data_as(ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)))
+    lens_p = lens.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    return arr, lens_p, (joined, base, ptrs, lens)
 
 
 class Context:
