@@ -1626,11 +1626,14 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
     int32_t *d_read_id = (int32_t *)(rb + off_bytes + len_bytes);
     b->d_reads = (uint8_t *)(rb + off_bytes + len_bytes + id_bytes);
     {
-      std::vector<char> host(b->reads_bytes);
-      int64_t *off = (int64_t *)host.data();
-      int32_t *ln = (int32_t *)(host.data() + off_bytes);
-      int32_t *ids = (int32_t *)(host.data() + off_bytes + len_bytes);
-      char *rd = host.data() + off_bytes + len_bytes + id_bytes;
+      // (not value-initialised: every byte up to the reads' end is written)
+      std::unique_ptr<char[]> host_buf(new char[b->reads_bytes]);
+      char *const host_data = host_buf.get();
+      std::memset(host_data + b->reads_bytes - 64, 0, 64);
+      int64_t *off = (int64_t *)host_data;
+      int32_t *ln = (int32_t *)(host_data + off_bytes);
+      int32_t *ids = (int32_t *)(host_data + off_bytes + len_bytes);
+      char *rd = host_data + off_bytes + len_bytes + id_bytes;
       int64_t at = 0;
       for (int64_t r = 0; r < n_reads; ++r) {
         const int64_t o = src[size_t(r)];
@@ -1640,7 +1643,10 @@ int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, con
         if (lens[o]) std::memcpy(rd + at, seqs[o], size_t(lens[o]));
         at += lens[o];
       }
-      CK(cudaMemcpyAsync(rb, host.data(), b->reads_bytes, cudaMemcpyHostToDevice, ctx->stream));
+      off[n_reads] = at;
+      ln[n_reads] = 0;
+      ids[n_reads] = 0;
+      CK(cudaMemcpyAsync(rb, host_data, b->reads_bytes, cudaMemcpyHostToDevice, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
       b->h2d_bytes = b->reads_bytes;
     }

@@ -46,12 +46,12 @@ def _seq_arrays(seqs: Seq[bytes]):
     joined into one buffer, each pointer its start in it (one copy of the
     bytes, no per-sequence objects). The third value keeps the buffers alive
     while the pointers are in use."""
-    seqs = [_bytes(s) for s in seqs]
+    seqs = [s if isinstance(s, bytes) else _bytes(s) for s in seqs]
     n = len(seqs)
     lens = np.fromiter((len(s) for s in seqs), dtype=np.int64, count=n)
     if n == 0:
         lens = np.zeros(1, dtype=np.int64)
-    joined = b"".join(seqs) + b"\0"
+    joined = b"".join(seqs + [b"\0"])  # (one copy: the terminator joins the list)
     base = np.frombuffer(joined, dtype=np.uint8)
     starts = np.zeros(max(1, n), dtype=np.uint64)
     if n > 1:
@@ -349,7 +349,7 @@ class Batch:
         self.ctx = ctx or default_context()
         self.L = self.ctx.L
         self.params = params
-        flat = [_bytes(s) for st in sets for s in st]
+        flat = [s if isinstance(s, bytes) else _bytes(s) for st in sets for s in st]
         off = [0]
         for st in sets:
             off.append(off[-1] + len(st))
