@@ -660,16 +660,22 @@ def main():
 
     # end to end through the C ABI from host buffers
     e2e_vals, h2d, d2h = [], 0, 0
+    e2e_parts = []
     out = None
     for _ in range(0 if args.no_e2e else max(1, min(args.steps, 2))):
         t0 = time.perf_counter()
         b2 = mp.Batch(params, sets, ctx)
+        t1 = time.perf_counter()
         st = b2.run(0)
+        t2 = time.perf_counter()
         out = b2.output_all(0)
+        t3 = time.perf_counter()
         h2d, d2h = b2.transfer_bytes()
         del b2
         dt = time.perf_counter() - t0
         e2e_vals.append(st.cells / dt / 1e9)
+        e2e_parts.append({"create_s": t1 - t0, "run_s": t2 - t1, "run_device_s": st.device_ms / 1e3,
+                          "output_s": t3 - t2, "release_s": t0 + dt - t3})
         assert out.count(b">consensus sequence\n") == len(sets)
     e2e_v = None
     if e2e_vals:
@@ -778,7 +784,8 @@ def main():
             "roofline_int": int_roof,
             "parity": parity,
             "cpu_baseline": cb,
-            "e2e": {"value": e2e_v, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_v, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "breakdown": e2e_parts[-1] if e2e_parts else None},
             "gpu_launches": launches,
             "clocks": clock_info,
             "plain_vs_batched": plain,
