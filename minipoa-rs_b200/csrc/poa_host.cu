@@ -1789,6 +1789,11 @@ int poa_batch_tune(poa_ctx *ctx, poa_batch *batch, int32_t warps_per_sm, uint64_
 int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *stats) {
   return api(ctx, [&] {
     if (mode != 0 && mode != 1) throw AlignError{POA_ERR_INVALID, "mode must be 0 (batched) or 1 (plain)"};
+    if (b->n_sets == 0) {  // nothing to align
+      if (stats) *stats = poa_batch_stats{};
+      b->ran = true;
+      return;
+    }
     // arena pool: the rest of the budget, allocated once
     if (!b->arenas) {
       // the other batches' pools are idle between their runs: take them back
@@ -1819,8 +1824,8 @@ int poa_batch_run(poa_ctx *ctx, poa_batch *b, int32_t mode, poa_batch_stats *sta
         // block per set, the set on warp 0 with three helper warps for its
         // DP rows, one arena per block (not with the row wavefront forced: a
         // warp leading helpers runs rows one at a time)
-        const bool team =
-            passes == 0 && b->giant_factor > 0 && int64_t(pending.size()) <= sms && b->P.row_wave != 2;
+        const bool team = passes == 0 && !pending.empty() && b->giant_factor > 0 &&
+                          int64_t(pending.size()) <= sms && b->P.row_wave != 2;
         if (team) slots = 4 * int64_t(pending.size());
         b->P.teams = team ? 1 : 0;
         int64_t slot_bytes = b->arena_pool / (team ? slots / 4 : slots) / 256 * 256;

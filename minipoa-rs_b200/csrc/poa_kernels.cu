@@ -261,6 +261,7 @@ cudaError_t launch_toposort(Job *job_dev, char *arena, int64_t bytes, cudaStream
 }
 
 cudaError_t launch_reset(Job *jobs_dev, int n_jobs, int sigma, int unknown, cudaStream_t stream) {
+  if (n_jobs <= 0) return cudaSuccess;
   k_reset<<<(n_jobs + 127) / 128, 128, 0, stream>>>(jobs_dev, n_jobs, sigma, unknown);
   return cudaGetLastError();
 }

@@ -257,6 +257,7 @@ cudaError_t launch_pack_one(const Job *job_dev, int n_nodes, int64_t *part, int3
 
 cudaError_t launch_pack(const Job *jobs_dev, const int32_t *ids, int n_ids, const int64_t *offsets, int32_t *out,
                         int sigma, cudaStream_t stream) {
+  if (n_ids <= 0) return cudaSuccess;
   const int threads = 128;
   const int blocks = (n_ids * 32 + threads - 1) / threads;
   k_pack<<<blocks, threads, 0, stream>>>(jobs_dev, ids, n_ids, offsets, out, sigma);

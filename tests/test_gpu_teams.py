@@ -56,3 +56,22 @@ def test_small_int32_batch_teams_match_the_oracle(mp, oracle, adaptive):
         o = oracle.align_sequences(params, reads)
         assert batch.graph(s).dump() == o.dump(5), f"set {s}"
         assert batch.output(s, 0) == ">consensus sequence\n" + o.consensus(params)[0].decode() + "\n"
+
+
+def test_empty_batch_and_tiny_sets(mp, oracle):
+    # no sets at all: nothing runs, nothing is output
+    empty = mp.Batch(Params(), [])
+    st = empty.run(0)
+    assert st.cells == 0
+    assert empty.output_all(0) == b""
+    del empty
+    # one-read sets and an empty read (src/graph.rs: a path of the unknown
+    # base only) as teams
+    params = Params()
+    sets = [[b"ACGTACGTTGCA"], [b""], [b"ACGT", b"ACGA", b""]]
+    batch = mp.Batch(params, sets)
+    batch.run(0)
+    for s, reads in enumerate(sets):
+        o = oracle.align_sequences(params, reads)
+        assert batch.graph(s).dump() == o.dump(5), f"set {s}"
+        assert batch.output(s, 0) == ">consensus sequence\n" + o.consensus(params)[0].decode() + "\n"
