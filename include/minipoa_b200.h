@@ -238,15 +238,17 @@ typedef struct poa_batch_stats {
   double device_ms;     /* device time of the last run (CUDA events) */
   int32_t launches;     /* kernel launches in the last run */
   int32_t relaunches;   /* extra passes for jobs that outgrew their DP arena */
-  int32_t slots;        /* concurrent warp slots of the first pass */
+  int32_t slots;        /* concurrent warp slots of the first pass (teams: 4 per set) */
   int32_t reserved;
   double kernel_ms;     /* device time inside the read-loop kernel launches */
   uint64_t dp_bytes;    /* DP state bytes stored (M, D, I per cell) */
   uint64_t pred_cells;  /* predecessor-cell updates: per row, the band overlap of each
                            in-band predecessor (align.rs:751-797 trip count) */
   uint64_t far_preds;   /* predecessor rows read from the arena, not the shared-memory ring */
-  uint64_t rows_g4;     /* DP rows of the 4-stripe tile (385-512 columns) */
-  uint64_t rows_generic;  /* DP rows of the generic row (wider, > 32 predecessors, i64) */
+  uint64_t rows_g4;     /* DP rows of more than 384 columns on the striped tiles (the wide
+                           kernel form: up to 2048 columns, in 512-column segments) */
+  uint64_t rows_generic;  /* DP rows of the generic row (wider than the striped tiles,
+                             > 32 predecessors, i64) */
   int32_t coop_jobs;    /* jobs that ran cooperative rows (a giant with helper warps) */
   int32_t wave_reads;   /* reads whose static-band DP ran as a row wavefront (lane per row) */
   uint64_t phase_cycles[4]; /* profiling builds only (POA_PHASE_CYCLES), else 0: warp cycles
@@ -259,7 +261,10 @@ typedef struct poa_batch_stats {
 int poa_batch_create(poa_ctx *ctx, const poa_params *params, int64_t n_sets, const int64_t *set_off,
                      const uint8_t *const *seqs, const int64_t *lens, poa_batch **out);
 /* Resets every set's graph to Graph::new and aligns all reads on the device.
- * Inputs already resident; returns after the device work completes. */
+ * Inputs already resident; returns after the device work completes. A batch
+ * of at most one set per SM runs as teams (one 4-warp block per set: the set
+ * and three helper warps on its DP rows); results are the same either way.
+ * A batch of no sets does nothing. */
 int poa_batch_run(poa_ctx *ctx, poa_batch *batch, int32_t mode, poa_batch_stats *stats);
 /* Per-set status after a run (0 = ok, else POA_ERR_ALIGN with message in
  * poa_batch_error). */
