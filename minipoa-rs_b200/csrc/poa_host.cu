@@ -961,11 +961,11 @@ std::vector<std::string> name_list(int64_t n, const char *const *names, const ch
 // ---------------------------------------------------------------------------
 // Batch of independent read sets.
 
-// Resident warps per SM of a batched run without a tuned setting: 6 of the
+// Resident warps per SM of a batched run without a tuned setting: 5 of the
 // kernel's 8 (the largest sets, which end the run, slow down when their SM
-// also runs four other jobs; measured 3.5-3.6 s per C3 step at 6 or 4 warps
-// per SM against 4.0-4.2 s at 8).
-constexpr int kDefaultBatchWarpsPerSm = 6;
+// also runs other jobs; the tuner picked 5 in most C3 runs, 3.16-3.21 s per
+// step, against 3.5-3.65 s at 6 and 4.0-4.2 s at 8).
+constexpr int kDefaultBatchWarpsPerSm = 5;
 
 struct poa_batch {
   poa_ctx *ctx = nullptr;
@@ -1733,7 +1733,7 @@ int poa_batch_autotune(poa_ctx *ctx, poa_batch *b, poa_batch_tuning *out) {
       int alone;
     };
     const Cand cand[] = {{kDefaultBatchWarpsPerSm, 1.5, 0}, {6, 1.5, 1}, {5, 1.5, 1}, {6, 1.0, 1}, {4, 1.5, 0},
-                         {5, 1.5, 0}, {7, 1.5, 0}, {8, 1.5, 0}, {8, 1.5, 1}};
+                         {6, 1.5, 0}, {7, 1.5, 0}, {8, 1.5, 0}, {8, 1.5, 1}};
     double best_ms = 0;
     Cand best{b->warps_per_sm, b->giant_factor, b->giant_alone};
     int tried = 0;
