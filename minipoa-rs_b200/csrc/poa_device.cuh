@@ -1549,7 +1549,7 @@ __device__ __forceinline__ void dp_row_fast(int lane, int start, int len, int32_
 // compose as carry[g+1] = max(aggregate[g], carry[g] + 128E).
 constexpr int COOP_ROWS = 0, COOP_DONE = 1;  // phase modes
 constexpr int COOP_GEN_MIN_LEN = 256;         // narrower int64 rows: the leader alone
-constexpr int COOP_ROW = 0, COOP_STOP = 1, COOP_GEN = 2;  // row operations
+constexpr int COOP_ROW = 0, COOP_STOP = 1, COOP_GEN = 2, COOP_SEG = 3;  // row operations
 struct CoopDesc {
   int mode, op, start, len, pos_i, n_pred, cap, pad0;
   int32_t E, O, pad1, pad2;
@@ -1557,7 +1557,7 @@ struct CoopDesc {
   const int32_t *mrow;
   const uint8_t *q8;
   int32_t *rm, *rd;
-  int32_t agg[4];
+  int32_t agg[16];  // per 512-column segment (COOP_SEG: up to 4), per stripe
   int ps[32], pl[32], pos[32];
   const int32_t *g[32];
   // int64 rows (COOP_GEN): per read, the gaps, the arena and the plan arrays;
@@ -1573,6 +1573,7 @@ struct CoopDesc {
 };
 static_assert(sizeof(CoopDesc) <= sizeof(int32_t) * RING_CAP, "CoopDesc must fit a ring array");
 __device__ inline void coop_gen64(CoopDesc *c, int g);
+__device__ inline void coop_seg(CoopDesc *c, int g);
 
 __device__ __forceinline__ void coop_bar(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 
@@ -1659,6 +1660,108 @@ __device__ inline void coop_stripe(CoopDesc *c, int g) {
   coop_bar(1);
 }
 
+// Cooperative rows of 513-2048 columns (the wide kernel forms): the row's
+// 512-column segments left to right, warp g computing stripe g of each (the
+// stripe arithmetic of coop_stripe). After a segment's stripes publish their
+// aggregates (barrier 1), each warp composes the insertion state entering
+// its stripe from the state entering the segment and the stripes before it,
+// and all warps carry the segment's four stripes into the next segment's
+// entry state. The row enters the ring only after every segment has read
+// its predecessors (each lane copies the columns it wrote; barrier 1 again
+// once the row is written), since a wide row's later segments may read
+// predecessor entries its earlier columns would overwrite.
+__device__ inline void coop_seg(CoopDesc *c, int g) {
+  const int lane = threadIdx.x & 31;
+  const int start = c->start, len = c->len, stop = start + len, cap = c->cap;
+  const int32_t E = c->E, O = c->O;
+  int32_t *rm = c->rm, *rd = c->rd;
+  int32_t *R = c->R;
+  const int np = c->n_pred;
+  const int nseg = (len + 511) / 512;
+  constexpr int32_t BELOW = INT32_MIN / 2;
+  int32_t entry = NEG32;  // insertion state entering the segment's first column
+  for (int sg = 0; sg < nseg; ++sg) {
+    const int j0 = start + 512 * sg + 128 * g + 4 * lane;
+    int32_t Mx[4], Dx[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      Mx[k] = NEG32;
+      Dx[k] = NEG32;
+    }
+    for (int t = 0; t < np; ++t) {
+      const int ps = c->ps[t], pl = c->pl[t], pos = c->pos[t];
+      const int32_t *gp = c->g[t];
+      const bool in = j0 < stop && j0 >= ps && j0 < ps + pl;
+      int4 m4, d4;
+      int32_t prev;
+      if (pos >= 0) {
+        const int x = ring_at(pos, ps, in ? j0 : ps, cap);
+        m4 = *reinterpret_cast<const int4 *>(rm + x);
+        d4 = *reinterpret_cast<const int4 *>(rd + x);
+        prev = rm[x == 0 ? cap - 1 : x - 1];
+      } else {
+        const int c0 = in ? j0 - ps : 0;
+        m4 = *reinterpret_cast<const int4 *>(gp + c0);
+        d4 = *reinterpret_cast<const int4 *>(gp + pl + c0);
+        prev = gp[c0 > 0 ? c0 - 1 : 0];
+      }
+      const int32_t pv = j0 > ps ? prev : NEG32;
+      if (in) {
+        Mx[0] = maxs(Mx[0], pv);
+        Mx[1] = maxs(Mx[1], m4.x);
+        Mx[2] = maxs(Mx[2], m4.y);
+        Mx[3] = maxs(Mx[3], m4.z);
+        Dx[0] = __viaddmax_s32(d4.x, E, __viaddmax_s32(m4.x, O, Dx[0]));
+        Dx[1] = __viaddmax_s32(d4.y, E, __viaddmax_s32(m4.y, O, Dx[1]));
+        Dx[2] = __viaddmax_s32(d4.z, E, __viaddmax_s32(m4.z, O, Dx[2]));
+        Dx[3] = __viaddmax_s32(d4.w, E, __viaddmax_s32(m4.w, O, Dx[3]));
+      }
+    }
+    int32_t X[4];
+    const uint32_t bw = *reinterpret_cast<const uint32_t *>(c->q8 + min(j0, stop - 4));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int32_t prof = c->mrow[(bw >> (8 * k)) & 0xff];
+      Mx[k] = __viaddmax_s32(Mx[k], prof, Dx[k]);  // Mx now holds md
+      X[k] = k == 0 ? Mx[k] + O : __viaddmax_s32(X[k - 1], E, Mx[k] + O);
+    }
+    int32_t y = X[3];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) y = __viaddmax_s32(__shfl_up_sync(FULL, y, d), d * 4 * E, y);
+    int32_t pre = __shfl_up_sync(FULL, y, 1);
+    if (lane == 0) pre = BELOW;
+    const int32_t y31 = __shfl_sync(FULL, y, 31);
+    if (lane == 0) c->agg[4 * sg + g] = y31;
+    coop_bar(1);
+    int32_t carry = entry;
+    for (int h = 0; h < g; ++h) carry = __viaddmax_s32(carry, 128 * E, c->agg[4 * sg + h]);
+    const int32_t cin = __viaddmax_s32(carry, 4 * lane * E, pre);
+    if (j0 < stop) {
+      int32_t iv[4], mv[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        iv[k] = k == 0 ? cin : __viaddmax_s32(cin, k * E, X[k - 1]);
+        mv[k] = maxs(Mx[k], iv[k]);
+      }
+      const int o = j0 - start;
+      *reinterpret_cast<int4 *>(R + o) = make_int4(mv[0], mv[1], mv[2], mv[3]);
+      *reinterpret_cast<int4 *>(R + len + o) = make_int4(Dx[0], Dx[1], Dx[2], Dx[3]);
+      *reinterpret_cast<int4 *>(R + 2 * len + o) = make_int4(iv[0], iv[1], iv[2], iv[3]);
+    }
+    for (int h = 0; h < 4; ++h) entry = __viaddmax_s32(entry, 128 * E, c->agg[4 * sg + h]);
+  }
+  for (int sg = 0; sg < nseg; ++sg) {
+    const int j0 = start + 512 * sg + 128 * g + 4 * lane;
+    if (j0 < stop) {
+      const int o = j0 - start;
+      const int x = ring_at(c->pos_i, start, j0, cap);
+      *reinterpret_cast<int4 *>(rm + x) = *reinterpret_cast<const int4 *>(R + o);
+      *reinterpret_cast<int4 *>(rd + x) = *reinterpret_cast<const int4 *>(R + len + o);
+    }
+  }
+  coop_bar(1);
+}
+
 // The block-mates' side: rows of every row loop the leader opens, until the
 // leader's job is done.
 __device__ inline void coop_helper(CoopDesc *c, int g) {
@@ -1673,6 +1776,8 @@ __device__ inline void coop_helper(CoopDesc *c, int g) {
       if (c->op == COOP_STOP) break;
       if (c->op == COOP_GEN)
         coop_gen64(c, g);
+      else if (c->op == COOP_SEG)
+        coop_seg(c, g);
       else
         coop_stripe(c, g);
     }
@@ -2634,7 +2739,7 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
         const int32_t *my_g = reinterpret_cast<const int32_t *>(A) + 3 * mcum;
         const unsigned vmask = __ballot_sync(FULL, ok);
         const int32_t *mrow = smem_matrix ? sm->matrix + base * P.sigma : P.matrix + base * P.sigma;
-        if (coop && len <= RING_MAX_LEN) {
+        if (coop) {
           const int slot = __popc(vmask & ((1u << lane) - 1u));
           if (ok) {
             cd->ps[slot] = mt.y;
@@ -2642,8 +2747,9 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
             cd->pos[slot] = mt.x < 0 ? -1 : mt.x;
             cd->g[slot] = my_g;
           }
+          const bool seg = len > RING_MAX_LEN;  // (the wide forms only)
           if (lane == 0) {
-            cd->op = COOP_ROW;
+            cd->op = seg ? COOP_SEG : COOP_ROW;
             cd->start = start;
             cd->len = len;
             cd->pos_i = pos_i;
@@ -2652,7 +2758,10 @@ __device__ int32_t poa_kernel(Job *J, const DevParams &P, char *arena, int64_t a
             cd->mrow = mrow;
           }
           coop_bar(1);
-          coop_stripe(cd, 0);  // the leader computes stripe 0
+          if (seg)
+            coop_seg(cd, 0);  // the leader computes stripe 0 of every segment
+          else
+            coop_stripe(cd, 0);  // the leader computes stripe 0
           continue;
         }
         int32_t bv = INT32_MIN;

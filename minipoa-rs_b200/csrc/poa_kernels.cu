@@ -71,18 +71,34 @@ __global__ void k_align(Job *J, DevParams P, char *arena, int64_t bytes, const u
   }
 }
 
-// The seed windows of one read (align.rs:99-164), one warp per window: warp w
-// aligns query[qbeg, qbeg + qlen) between anchor nodes beg (included) and
-// end (excluded) with the full-DP retry, in its own arena slice, and writes
-// its path to items[item_off[w] ...]. The graph is only read.
+// The seed windows of one read (align.rs:99-164), one 4-warp team per
+// window: block w aligns query[qbeg, qbeg + qlen) between anchor nodes beg
+// (included) and end (excluded) with the full-DP retry, in its own arena
+// slice, and writes its path to items[item_off[w] ...]; warp 0 runs the
+// alignment and warps 1-3 help with its DP rows (cooperative rows, their
+// shared memory the ring). The graph is only read.
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
     k_windows(Job *J, DevParams P, char *arenas, int64_t slot_bytes, int n_win, const int4 *win,
               const uint64_t *band, const uint8_t *query, int4 *items, const int64_t *item_off, int32_t *out_n,
               int32_t *out_st) {
   const int lane = threadIdx.x & 31;
-  const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t w = blockIdx.x;
   if (w >= n_win) return;
-  ring_default(warp_smem());
+  WarpSmem *sm = warp_smem();
+  ring_default(sm);
+  const int me = int(threadIdx.x >> 5);
+  if (me > 0) {  // a helper: rows of the window's row loops until released
+    coop_helper(reinterpret_cast<CoopDesc *>((sm - me)->ring_m), me);
+    return;
+  }
+  if (lane == 0) {
+    const int cap = int(3 * sizeof(WarpSmem) / 8 / 8 * 8);
+    sm->rv.m = reinterpret_cast<int32_t *>(sm + 1);
+    sm->rv.d = reinterpret_cast<int32_t *>(sm + 1) + cap;
+    sm->rv.cap = cap;
+    sm->rv.pad[0] = 1;  // cooperative rows
+  }
+  __syncwarp();
   const int4 d = win[w];  // (beg, end, qbeg, qlen | adaptive << 31)
   const bool adaptive = (unsigned(d.w) >> 31) != 0;
   const int qlen = d.w & 0x7fffffff;
@@ -90,7 +106,8 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, BLOCKS_PER_SM)
   int n_items = 0;
   Work cells{};
   const int32_t st = poa_retry<true>(J, P, arenas + w * slot_bytes, slot_bytes, d.x, d.y, query + d.z, qlen, adaptive,
-                               band[w], s, &n_items, &cells, warp_smem());
+                               band[w], s, &n_items, &cells, sm);
+  coop_release(sm);  // the helpers leave
   if (st == ST_OK)
     for (int k = lane; k < n_items; k += 32) items[item_off[w] + k] = s.items[k];
   if (lane == 0) {
@@ -233,9 +250,16 @@ cudaError_t launch_windows(Job *job_dev, const DevParams &P, char *arenas, int64
                            const int4 *win, const uint64_t *band, const uint8_t *query, int4 *items,
                            const int64_t *item_off, int32_t *out_n, int32_t *out_st, cudaStream_t stream) {
   if (n_win <= 0) return cudaSuccess;
-  // one warp per block: the windows of a launch spread over all SMs
-  k_windows<<<n_win, 32, sizeof(WarpSmem), stream>>>(job_dev, P, arenas, slot_bytes, n_win, win, band, query, items,
-                                                     item_off, out_n, out_st);
+  // one 4-warp team per window (the window's warp and three helpers)
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(4 * sizeof(WarpSmem)));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_windows<<<n_win, 4 * 32, 4 * sizeof(WarpSmem), stream>>>(job_dev, P, arenas, slot_bytes, n_win, win, band, query,
+                                                             items, item_off, out_n, out_st);
   return cudaGetLastError();
 }
 
